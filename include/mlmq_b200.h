@@ -1,0 +1,202 @@
+/*
+ * mlmq_b200.h -- C ABI of libmlmq_b200.so, the B200 (sm_100a) delta-stepping
+ * single-source shortest-path solver.
+ *
+ * Two groups of entry points:
+ *
+ *  1. The reference solver's own entry points, kept with the same names,
+ *     argument meaning and index conventions so the library is a drop-in for
+ *     the reference's single-GPU solver (hideoze/mlmq_tpds_withl3,
+ *     evidence/l3_supplement_20260921_v2/single_source/SSSP/sssp_run.cu):
+ *     sssp_init, sssp_re_init, sssp_run_adaptive, sssp_cp_data.  They are
+ *     exported twice: with C linkage (declared here) and with the reference's
+ *     C++ linkage (declared in sssp_drop_in.h) so the reference's own caller,
+ *     SS/SSSP/main.cu, links against this library unchanged.
+ *
+ *  2. The library's own mlmq_* API: host graph generators and .gr I/O,
+ *     device graphs, a re-entrant solver context, the batched multi-source
+ *     solver and the serving loop.
+ *
+ * Conventions: vertex ids are 0-based; distances are int32 with INT_MAX
+ * (0x7FFFFFFF) meaning unreachable, as in the reference (core/include/
+ * common.h:11-20, VALUE_TYPE=int, DIST_MAX=INT_MAX); edge weights must be
+ * non-negative and every finite distance must be < INT_MAX.  Every function
+ * returns 0 on success or a negative MLMQ_ERR_* code; none calls exit().
+ */
+#ifndef MLMQ_B200_H
+#define MLMQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------ */
+#define MLMQ_OK 0
+#define MLMQ_ERR_CUDA (-1)        /* a CUDA runtime call failed */
+#define MLMQ_ERR_ARG (-2)         /* invalid argument */
+#define MLMQ_ERR_TIMEOUT (-3)     /* a device-side wait ran past its limit */
+#define MLMQ_ERR_QUEUE_FULL (-4)  /* a queue ring stayed full past its limit */
+#define MLMQ_ERR_STATE (-5)       /* call out of order (e.g. run before init) */
+#define MLMQ_ERR_NOMEM (-6)       /* host or device allocation failed */
+#define MLMQ_ERR_UNSUPPORTED (-7) /* configuration not built in this library */
+#define MLMQ_ERR_RANGE (-8)       /* a distance sum reached INT_MAX */
+#define MLMQ_ERR_IO (-9)          /* file open/read/write or format error */
+#define MLMQ_ERR_NODEV (-10)      /* no CUDA device, or not sm_100 */
+#define MLMQ_ERR_BUSY (-11)       /* serving: no free slot or memory now */
+#define MLMQ_ERR_MISMATCH (-12)   /* sssp_run_adaptive: result differs from the
+                                     caller's CPU distances (node_data_base) */
+
+/* Human-readable name of an MLMQ_ERR_* code. */
+const char *mlmq_strerror(int code);
+
+/* ---- queue configuration (reference: core/include/adaptive.h:5-62) ----- */
+
+/* Queue types, numbered as the reference's enum mlmq_type
+ * (core/include/common.h:85-108).  This library implements L1SLF_L2DQ (the
+ * type the reference's timed path forces, sssp_run.cu:895) and L1V_L2DQ. */
+#define MLMQ_L1V_L2DQ 0
+#define MLMQ_L1SLF_L2DQ 19
+
+typedef struct mlmq_config {
+    int queue_type;      /* MLMQ_L1SLF_L2DQ (default) or MLMQ_L1V_L2DQ */
+    int delta;           /* bucket width; reference BENCH_DELTA, default 200000 */
+    int work_blocks;     /* persistent CTAs; 0 = one per SM that fits
+                            (reference MLMQ_WORK_BLOCKS) */
+    int warps_per_block; /* worker warps per CTA (reference: 512 threads = 16) */
+    int l2_batch;        /* slots claimed per bucket read (l2_batch_size, 8) */
+    int bucket_num;      /* L2 buckets (BNUM, 16; at most 32) */
+    int bucket_max;      /* buckets readable at once (BUCKET_MAX, 4) */
+    int min_read;        /* records wanted per read (MIN_READ_GRA, 8) */
+    int large_degree;    /* warp-cooperative relaxation at this out-degree
+                            (LARGEV, 16) */
+    int l1_spill;        /* L1 spills to L2 when it holds more (32) */
+    int l2_cap_log2;     /* log2 slots per L2 bucket ring; 0 = sized from graph */
+    int l3_cap_log2;     /* log2 slots of the L3 ring; 0 = sized from graph */
+    int timeout_ms;      /* device wait limit per solve (default 20000) */
+} mlmq_config;
+
+/* Fills *cfg with the reference's defaults (common.h:24-34, sssp.cuh:20,
+ * sssp_run.cu:896) and then applies the environment overrides the reference
+ * reads: BENCH_DELTA, BENCH_QUEUE, MLMQ_WORK_BLOCKS. */
+int mlmq_config_default(mlmq_config *cfg);
+
+/* ---- 1. reference entry points (C linkage) ---------------------------- */
+
+/* Layout-compatible with the reference's struct graph_info
+ * (core/include/graph_info.h:8-22); passed by value, read-only. */
+typedef struct graph_info {
+    int m;
+    int nnz;
+    float avg_nnz;
+    float max_nnz;
+    float dev_nnz;
+    float avg_weight;
+    float dev_weight;
+    float max_weight;
+    float diameter;
+} graph_info;
+
+/* SS/SSSP/sssp_run.cu:676.  Binds a caller-owned DEVICE CSR: m vertices,
+ * nnz arcs, RowPtr[m+1], ColIdx[nnz] (0-based), edge_data[nnz].  Allocates
+ * the distance array and queue storage on the current device. */
+int sssp_init(int m, int nnz, int *RowPtr, int *ColIdx, int *edge_data);
+/* SS/SSSP/sssp_run.cu:709.  Resets every distance to INT_MAX. */
+int sssp_re_init(void);
+/* SS/SSSP/sssp_run.cu:888.  Solves from 0-based src with the configuration
+ * of mlmq_config_default().  Like the reference it runs BENCH_WARMUPS (2)
+ * untimed and BENCH_REPEATS (3) timed solves and prints one
+ * "BENCH algorithm=MLMQ ..." line per solve. */
+int sssp_run_adaptive(int src, graph_info info);
+/* SS/SSSP/sssp_run.cu:749.  *node_data_h receives a malloc()ed host array of
+ * m distances (0-based) that the caller frees. */
+int sssp_cp_data(int **node_data_h);
+
+/* ---- 2a. host graphs -------------------------------------------------- */
+
+typedef struct mlmq_host_graph mlmq_host_graph;
+
+/* width x height 4-neighbour grid, id = y*width + x; each undirected edge is
+ * dropped with probability drop_p (seeded Bernoulli); both arcs share one
+ * weight uniform in [wmin, wmax]. */
+int mlmq_hgraph_grid(int width, int height, double drop_p, int wmin, int wmax,
+                     uint64_t seed, mlmq_host_graph **out);
+/* npoints uniform in the unit square joined to their k nearest neighbours,
+ * symmetrised, weight = round(scale * euclid) + 1; vertex ids follow a
+ * Morton order of a cell grid; perm[id] = index of the generated point. */
+int mlmq_hgraph_knn(int npoints, int k, double scale, uint64_t seed,
+                    mlmq_host_graph **out);
+/* R-MAT: 2^scale vertices, edge_factor * 2^scale sampled directed arcs with
+ * quadrant probabilities (a, b, c, 1-a-b-c); self-loops and duplicates
+ * removed; weight uniform in [wmin, wmax]. */
+int mlmq_hgraph_rmat(int scale, int edge_factor, double a, double b, double c,
+                     int wmin, int wmax, uint64_t seed, mlmq_host_graph **out);
+/* Copies a host CSR (validated like the reference exporter,
+ * scripts/multigpu/supplement_graph.cpp:21-28). */
+int mlmq_hgraph_from_csr(int n, int64_t m, const int *row, const int *col,
+                         const int *w, mlmq_host_graph **out);
+/* Galois/LonestarGPU .gr v1 (SSSP/csr_graph.cu:185-300, 302-418). */
+int mlmq_hgraph_read_gr(const char *path, mlmq_host_graph **out);
+int mlmq_hgraph_write_gr(const mlmq_host_graph *g, const char *path);
+/* Borrowed views; valid until mlmq_hgraph_free.  perm may be NULL. */
+int mlmq_hgraph_view(const mlmq_host_graph *g, int *n, int64_t *m, const int **row,
+                     const int **col, const int **w, const int **perm);
+void mlmq_hgraph_free(mlmq_host_graph *g);
+
+/* ---- 2b. device graphs and the solver context ------------------------- */
+
+typedef struct mlmq_graph mlmq_graph;
+typedef struct mlmq_solver mlmq_solver;
+
+/* Copies a host CSR to the current device (pinned staging) and builds the
+ * interleaved {dst, weight} arc array the kernels read. */
+int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
+                      mlmq_graph **out);
+/* Wraps a caller-owned device CSR (not copied; must outlive the graph). */
+int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
+                           const int *d_w, mlmq_graph **out);
+int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m);
+void mlmq_graph_free(mlmq_graph *g);
+
+/* A solver owns one distance array and one queue workspace on the device
+ * current at creation.  cfg may be NULL (mlmq_config_default). */
+int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg, mlmq_solver **out);
+/* Enqueues one complete solve from src on `stream` (a cudaStream_t; NULL =
+ * the solver's own stream): distance reset, seed, persistent kernel.
+ * Returns after the launch; mlmq_solver_wait reports the outcome. */
+int mlmq_solver_launch(mlmq_solver *s, int src, void *stream);
+/* Blocks until the last launch ends; returns its status as MLMQ_ERR_*. */
+int mlmq_solver_wait(mlmq_solver *s);
+/* launch + wait. */
+int mlmq_solver_solve(mlmq_solver *s, int src);
+/* Device pointer to the n distances of the last solve. */
+int mlmq_solver_dist(mlmq_solver *s, int **d_dist);
+/* Copies the n distances to host memory (synchronous). */
+int mlmq_solver_copy_dist(mlmq_solver *s, int *h_dist);
+
+typedef struct mlmq_solve_stats {
+    uint64_t pushed;     /* records written to L2/L3 */
+    uint64_t l3_pushed;  /* of which to the L3 ring */
+    uint64_t relaxed;    /* arcs scanned */
+    uint64_t improved;   /* successful atomicMin updates */
+    uint32_t first_max;  /* last bucket index reached */
+    int grid;            /* persistent CTAs launched */
+    int block;           /* threads per CTA */
+    uint32_t status;     /* raw device status word */
+} mlmq_solve_stats;
+int mlmq_solver_stats(mlmq_solver *s, mlmq_solve_stats *st);
+void mlmq_solver_destroy(mlmq_solver *s);
+
+/* One-shot host-buffer call: upload the CSR, solve every source in srcs one
+ * after another, copy each distance array to h_dist (nsrc x n, row-major).
+ * This is the whole user-facing path with host buffers. */
+int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
+                    int nsrc, const int *srcs, int *h_dist, const mlmq_config *cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLMQ_B200_H */

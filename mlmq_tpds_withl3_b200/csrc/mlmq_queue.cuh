@@ -1,0 +1,430 @@
+// mlmq_queue.cuh -- the three-level MLMQ work queue and the CSR relaxation
+// step, as warp-cooperative device functions used by the persistent kernel.
+//
+// Reference behaviour restated here (hideoze/mlmq_tpds_withl3):
+//  * L1 SLF queue, core/src/l1_queue.cu:218-360: a 64-slot ring per warp in
+//    shared memory; an incoming record goes to the FRONT when its distance is
+//    below the front record's (or, with the ring empty, below the first
+//    incoming record's), otherwise to the BACK; when the ring holds more than
+//    32 records every record spills to L2; reads take up to 32 from the front.
+//  * L2 delta buckets, core/cu_delta_queue/cu_delta_queue.cuh:78-642: BNUM
+//    circular buckets of width delta starting at bucket `first`; writers
+//    reserve slots with one warp-aggregated atomicAdd per destination bucket
+//    (__match_any_sync); readers claim l2_batch_size slots per bucket from up
+//    to BUCKET_MAX buckets starting at `first`, keep a claim they could not
+//    finish, and stop once MIN_READ_GRA records are held; `first` moves on
+//    once its bucket is empty and other buckets still hold records.
+//  * Relaxation, SS/SSSP/sssp_run.cu:143-413: stale records (distance above
+//    the vertex's current distance) are dropped; vertices of out-degree >=
+//    LARGEV are relaxed by the whole warp, smaller ones through a warp prefix
+//    sum over degrees that gives every lane one arc; atomicMin on int32
+//    distances; winners are ballot-compacted into the queue.
+//  * Termination, sssp_run.cu:565-572 and :644-661: a warp returns the read
+//    credit of its L2 records only when its L1 is empty, and the solve ends
+//    when (records reserved) - (credit returned) reaches zero.
+//
+// Where the B200 design differs (each a deliberate change, not a port):
+//  * Publication without manager warps.  A ring slot is one 64-bit word
+//    holding the record plus a 2-bit lap tag; the writer installs it with one
+//    atomicCAS from the empty word, so a reader knows a slot is readable from
+//    the slot alone and clears it after reading.  The reference needed
+//    per-512-record write counters and 16 manager warps to publish read_pos.
+//  * Per-CTA mirror.  One warp per CTA copies the queue counters into shared
+//    memory; worker warps poll that copy instead of global memory, so idle
+//    warps add no global traffic.
+//  * Urgent bucket.  A record whose distance is below the window start (it
+//    was produced while `first` moved on) goes to one extra ring that readers
+//    visit first, instead of being clamped into bucket `first`, whose ring
+//    may already stand for a far bucket.
+//  * L3.  Records beyond the bucket window (the reference clamps them into
+//    the last bucket) and records for a bucket whose ring is filling go to
+//    one HBM ring shared by every CTA.  Warps read it when every L2 bucket is
+//    empty and move `first` up to the batch they took.
+//  * Every wait is bounded by a deadline and ends with a status bit, never a
+//    trap or an endless spin.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace mlmq {
+
+struct PlainParams {
+    int n;
+    const int *__restrict__ row;
+    const int2 *__restrict__ arcs;  // interleaved {dst, weight}
+    int *dist;
+    int src;
+    unsigned long long *l2;  // (nb + 1) rings of 2^l2_log slots; ring nb is the urgent ring
+    unsigned long long *l3;  // 2^l3_log slots
+    unsigned *ctlw;
+    int nb, bm, batch, min_read, large, l1_spill, l1_vector;
+    unsigned delta;
+    int l2_log, l3_log;
+    int workers;  // worker warps per CTA (one more warp per CTA is the manager)
+    unsigned long long timeout_ns;
+};
+
+// Shared-memory copy of the global queue counters, refreshed by the manager
+// warp of each CTA.
+struct Mirror {
+    unsigned first, exit, pressure;
+    unsigned l3_reserve, l3_claim, l3_consumed;
+    unsigned reserve[NB_MAX], claim[NB_MAX], consumed[NB_MAX];
+};
+
+// Per-warp queue state held in registers.  l1_* and the L3 claim are
+// warp-uniform; c_lo/c_hi are lane-distributed (lane b: claim on ring b).
+struct WarpQ {
+    int l1_head, l1_tail, l1_size;
+    unsigned c_lo, c_hi;
+    unsigned l3_lo, l3_hi;
+    unsigned onfly;
+    unsigned idle_ns;
+    unsigned range_hit;
+    unsigned long long pushed, l3_pushed, relaxed, improved;
+    unsigned long long deadline;
+};
+
+__device__ __forceinline__ unsigned long long *l2_slot(const PlainParams &p, int ring, unsigned s) {
+    return p.l2 + ((size_t)ring << p.l2_log) + (s & ((1u << p.l2_log) - 1u));
+}
+__device__ __forceinline__ unsigned long long *l3_slot(const PlainParams &p, unsigned s) {
+    return p.l3 + (s & ((1u << p.l3_log) - 1u));
+}
+
+__device__ __forceinline__ void raise_status(const PlainParams &p, unsigned bits) {
+    atomicOr(p.ctlw + ctl::STATUS, bits);
+    st_relaxed(p.ctlw + ctl::EXIT, 1u);
+}
+
+// Installs a record in a slot still holding the previous lap's record: waits,
+// bounded by the deadline, for its reader to clear it.
+static __device__ __noinline__ void install_slow(const PlainParams &p, unsigned long long *slot,
+                                          unsigned long long rec, unsigned long long deadline) {
+    unsigned ns = 64;
+    for (;;) {
+        __nanosleep(ns);
+        if (atomicCAS(slot, SENT, rec) == SENT) return;
+        if (ns < 2048) ns <<= 1;
+        if (globaltimer() > deadline || ld_relaxed(p.ctlw + ctl::EXIT)) {
+            raise_status(p, ST_QUEUE_FULL);
+            return;
+        }
+    }
+}
+
+// Warp-cooperative push of up to 32 records (one per lane with `valid`).
+// Ring choice: urgent ring for distances below the window, bucket
+// floor(d/delta) mod nb inside the window, L3 beyond it or under pressure.
+__device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool valid, unsigned v,
+                                       unsigned d) {
+    const unsigned act = __ballot_sync(FULL, valid);
+    if (!act) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned f = ld_relaxed(p.ctlw + ctl::FIRST);
+    const unsigned pres = ld_relaxed(p.ctlw + ctl::PRESSURE);
+    int tgt = -1;
+    if (valid) {
+        const unsigned L = d / p.delta;
+        if (L < f) {
+            tgt = p.nb;  // urgent ring
+        } else if (L - f >= (unsigned)p.nb) {
+            tgt = NB_MAX;  // L3
+        } else {
+            const int b = (int)(L % (unsigned)p.nb);
+            tgt = ((pres >> b) & 1u) ? NB_MAX : b;
+        }
+    }
+    const unsigned grp = __match_any_sync(FULL, tgt);
+    const int leader = __ffs(grp) - 1;
+    const unsigned rank = __popc(grp & lanemask_lt());
+    const unsigned cnt = __popc(grp);
+    unsigned base = 0;
+    if (valid && lane == leader) {
+        if (tgt < NB_MAX) {
+            const unsigned cons = ld_relaxed(p.ctlw + ctl::CONSUMED + tgt);
+            base = atomicAdd(p.ctlw + ctl::RESERVE + tgt, cnt);
+            if (base + cnt - cons > (1u << (p.l2_log - 1)) && tgt < p.nb)
+                atomicOr(p.ctlw + ctl::PRESSURE, 1u << tgt);
+        } else {
+            base = atomicAdd(p.ctlw + ctl::L3_RESERVE, cnt);
+        }
+    }
+    base = __shfl_sync(FULL, base, leader);
+    if (valid) {
+        const unsigned s = base + rank;
+        unsigned long long *slot;
+        unsigned lap;
+        if (tgt < NB_MAX) {
+            slot = l2_slot(p, tgt, s);
+            lap = s >> p.l2_log;
+        } else {
+            slot = l3_slot(p, s);
+            lap = s >> p.l3_log;
+        }
+        const unsigned long long rec = rec_pack(v, d, lap);
+        if (atomicCAS(slot, SENT, rec) != SENT) install_slow(p, slot, rec, q.deadline);
+    }
+    const unsigned l3m = __ballot_sync(FULL, valid && tgt == NB_MAX);
+    q.pushed += __popc(act);
+    q.l3_pushed += __popc(l3m);
+}
+
+// ---- L1: warp-private ring in shared memory ---------------------------------
+// SLF insert (l1_queue.cu:284-330) or, for the vector L1, append at the back;
+// then spill everything to L2 when more than l1_spill records are held
+// (l1_queue.cu:332-350).  At most 32 records per call, so the 64-slot ring
+// never overflows.
+__device__ __forceinline__ void l1_write(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
+                                         unsigned v, unsigned d) {
+    const unsigned vm = __ballot_sync(FULL, valid);
+    if (!vm) return;
+    const unsigned front_d =
+        q.l1_size > 0 ? ring[q.l1_head].y : __shfl_sync(FULL, d, __ffs(vm) - 1);
+    const bool left = valid && !p.l1_vector && d < front_d;
+    const unsigned lm = __ballot_sync(FULL, left);
+    const unsigned rm = vm & ~lm;
+    if (left)
+        ring[(q.l1_head - (int)__popc(lm & lanemask_le())) & (L1_CAP - 1)] = make_uint2(v, d);
+    else if (valid)
+        ring[(q.l1_tail + (int)__popc(rm & lanemask_lt())) & (L1_CAP - 1)] = make_uint2(v, d);
+    __syncwarp();
+    q.l1_head = (q.l1_head - (int)__popc(lm)) & (L1_CAP - 1);
+    q.l1_tail = (q.l1_tail + (int)__popc(rm)) & (L1_CAP - 1);
+    q.l1_size += (int)__popc(vm);
+    if (q.l1_size > p.l1_spill) {
+        const int lane = threadIdx.x & 31;
+        for (int c = 0; c < q.l1_size; c += 32) {
+            const int i = c + lane;
+            const bool ok = i < q.l1_size;
+            uint2 it = make_uint2(0u, 0u);
+            if (ok) it = ring[(q.l1_head + i) & (L1_CAP - 1)];
+            push32(p, q, ok, it.x, it.y);
+        }
+        __syncwarp();
+        q.l1_head = q.l1_tail;
+        q.l1_size = 0;
+    }
+}
+
+// Up to 32 records from the front of L1 (l1_queue.cu:253-273).
+__device__ __forceinline__ void l1_read(WarpQ &q, const uint2 *ring, bool &valid, unsigned &v,
+                                        unsigned &d) {
+    const int lane = threadIdx.x & 31;
+    const int k = q.l1_size < 32 ? q.l1_size : 32;
+    valid = lane < k;
+    if (valid) {
+        const uint2 it = ring[(q.l1_head + lane) & (L1_CAP - 1)];
+        v = it.x;
+        d = it.y;
+    }
+    __syncwarp();
+    q.l1_head = (q.l1_head + k) & (L1_CAP - 1);
+    q.l1_size -= k;
+}
+
+// Takes the readable prefix of this warp's claim on L2 ring `ring` into
+// inb[got...]; returns the number taken.
+__device__ __forceinline__ int take_claim(const PlainParams &p, volatile Mirror &mir, int ring,
+                                          unsigned &lo, unsigned hi, uint2 *inb, int got) {
+    const int lane = threadIdx.x & 31;
+    const unsigned res = mir.reserve[ring];
+    int ready = (int)(res - lo);
+    if (ready <= 0) return 0;
+    if (ready > (int)(hi - lo)) ready = (int)(hi - lo);
+    if (ready > 32 - got) ready = 32 - got;
+    unsigned long long r = SENT;
+    bool ok = false;
+    const unsigned s = lo + lane;
+    if (lane < ready) {
+        r = ld_relaxed64(l2_slot(p, ring, s));
+        ok = (r != SENT) && rec_lap(r) == ((s >> p.l2_log) & 3u);
+    }
+    const unsigned okm = __ballot_sync(FULL, ok);
+    int take = (okm == FULL) ? 32 : (__ffs(~okm) - 1);
+    if (take > ready) take = ready;
+    if (lane < take) {
+        inb[got + lane] = make_uint2(rec_v(r), rec_d(r));
+        st_relaxed64(l2_slot(p, ring, s), SENT);
+    }
+    if (take > 0 && lane == 0) atomicAdd(p.ctlw + ctl::CONSUMED + ring, (unsigned)take);
+    lo += (unsigned)take;
+    return take;
+}
+
+// One ring of the read window: continue a pending claim or make a new one
+// (only when the mirror shows unclaimed reserved slots), then take records.
+__device__ __forceinline__ int read_ring(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
+                                         int ring, uint2 *inb, int got) {
+    const int lane = threadIdx.x & 31;
+    unsigned lo = __shfl_sync(FULL, q.c_lo, ring);
+    unsigned hi = __shfl_sync(FULL, q.c_hi, ring);
+    if (lo == hi) {
+        if ((int)(mir.reserve[ring] - mir.claim[ring]) <= 0) return 0;
+        if (got + p.batch > 32) return 0;
+        unsigned nlo = 0;
+        if (lane == 0) {
+            nlo = atomicAdd(p.ctlw + ctl::CLAIM + ring, (unsigned)p.batch);
+            atomicMax((unsigned *)&mir.claim[ring], nlo + (unsigned)p.batch);
+        }
+        lo = __shfl_sync(FULL, nlo, 0);
+        hi = lo + (unsigned)p.batch;
+    }
+    const int t = take_claim(p, mir, ring, lo, hi, inb, got);
+    if (lane == ring) {
+        q.c_lo = lo;
+        q.c_hi = hi;
+    }
+    return t;
+}
+
+// L2 read (cu_delta_queue.cuh:272-428 with ml_queue.cu:238-307): urgent ring
+// first, then buckets first .. first+bucket_max-1, until min_read records.
+__device__ __forceinline__ int l2_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
+                                       uint2 *inb) {
+    int got = read_ring(p, q, mir, p.nb, inb, 0);
+    const unsigned f = mir.first;
+    for (int i = 0; i < p.bm && got < p.min_read; i++) {
+        const int b = (int)((f + (unsigned)i) % (unsigned)p.nb);
+        got += read_ring(p, q, mir, b, inb, got);
+    }
+    return got;
+}
+
+// L3 read: only when every L2 ring is empty.  Takes up to 32 records and
+// moves `first` up to the smallest bucket among them.
+__device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
+                                       uint2 *inb) {
+    const int lane = threadIdx.x & 31;
+    unsigned pending = 0;
+    if (lane <= p.nb) pending = mir.reserve[lane] - mir.consumed[lane];
+    if (__ballot_sync(FULL, pending != 0)) return 0;
+    if (q.l3_lo == q.l3_hi) {
+        if ((int)(mir.l3_reserve - mir.l3_claim) <= 0) return 0;
+        unsigned nlo = 0;
+        if (lane == 0) {
+            nlo = atomicAdd(p.ctlw + ctl::L3_CLAIM, 32u);
+            atomicMax((unsigned *)&mir.l3_claim, nlo + 32u);
+        }
+        q.l3_lo = __shfl_sync(FULL, nlo, 0);
+        q.l3_hi = q.l3_lo + 32u;
+    }
+    int ready = (int)(mir.l3_reserve - q.l3_lo);
+    if (ready <= 0) return 0;
+    if (ready > (int)(q.l3_hi - q.l3_lo)) ready = (int)(q.l3_hi - q.l3_lo);
+    const unsigned s = q.l3_lo + lane;
+    unsigned long long r = SENT;
+    bool ok = false;
+    if (lane < ready) {
+        r = ld_relaxed64(l3_slot(p, s));
+        ok = (r != SENT) && rec_lap(r) == ((s >> p.l3_log) & 3u);
+    }
+    const unsigned okm = __ballot_sync(FULL, ok);
+    int take = (okm == FULL) ? 32 : (__ffs(~okm) - 1);
+    if (take > ready) take = ready;
+    unsigned dmin = 0xffffffffu;
+    if (lane < take) {
+        inb[lane] = make_uint2(rec_v(r), rec_d(r));
+        st_relaxed64(l3_slot(p, s), SENT);
+        dmin = rec_d(r);
+    }
+    if (take > 0) {
+        for (int o = 16; o > 0; o >>= 1) dmin = min(dmin, __shfl_xor_sync(FULL, dmin, o));
+        if (lane == 0) {
+            atomicAdd(p.ctlw + ctl::L3_CONSUMED, (unsigned)take);
+            atomicMax(p.ctlw + ctl::FIRST, dmin / p.delta);
+        }
+    }
+    q.l3_lo += (unsigned)take;
+    return take;
+}
+
+// ---- relaxation --------------------------------------------------------------
+__device__ __forceinline__ bool relax_arc(const PlainParams &p, WarpQ &q, unsigned dst,
+                                          unsigned nd) {
+    const int cur = __ldcg(p.dist + dst);
+    if (nd >= (unsigned)INT_MAX) {
+        if (cur == INT_MAX) q.range_hit = 1;
+        return false;
+    }
+    if ((int)nd >= cur) return false;
+    const int old = atomicMin(p.dist + dst, (int)nd);
+    if ((int)nd < old) {
+        q.improved++;
+        return true;
+    }
+    return false;
+}
+
+// Relaxes up to 32 records (one per lane) and feeds the winners to L1.
+__device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
+                                            unsigned v, unsigned d) {
+    const int lane = threadIdx.x & 31;
+    int beg = 0, deg = 0;
+    unsigned du = 0;
+    if (valid) {
+        const int cur = __ldcg(p.dist + v);
+        if ((int)d <= cur) {
+            du = (unsigned)cur;
+            beg = __ldg(p.row + v);
+            deg = __ldg(p.row + v + 1) - beg;
+        }
+    }
+    q.relaxed += (unsigned)deg;
+    // Whole-warp relaxation of large vertices (sssp_run.cu:192-265).
+    unsigned big = __ballot_sync(FULL, deg >= p.large);
+    while (big) {
+        const int sl = __ffs(big) - 1;
+        big &= big - 1;
+        const int lb = __shfl_sync(FULL, beg, sl);
+        const int ld = __shfl_sync(FULL, deg, sl);
+        const unsigned lu = __shfl_sync(FULL, du, sl);
+        for (int e0 = 0; e0 < ld; e0 += 32) {
+            const int e = e0 + lane;
+            bool win = false;
+            unsigned dst = 0, nd = 0;
+            if (e < ld) {
+                const int2 a = __ldg(p.arcs + lb + e);
+                dst = (unsigned)a.x;
+                nd = lu + (unsigned)a.y;
+                win = relax_arc(p, q, dst, nd);
+            }
+            l1_write(p, q, ring, win, dst, nd);
+        }
+    }
+    if (deg >= p.large) deg = 0;
+    // Small vertices: one arc per lane through an exclusive prefix sum of
+    // degrees (sssp_run.cu:269-379); the owner lane of arc e is the last lane
+    // whose offset is <= e, found by a 5-step shuffle search.
+    int incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const int off = incl - deg;
+    for (int e0 = 0; e0 < total; e0 += 32) {
+        const int e = e0 + lane;
+        int j = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const int oc = __shfl_sync(FULL, off, j + s);
+            if (oc <= e) j += s;
+        }
+        const int ob = __shfl_sync(FULL, beg, j);
+        const int oo = __shfl_sync(FULL, off, j);
+        const unsigned ou = __shfl_sync(FULL, du, j);
+        bool win = false;
+        unsigned dst = 0, nd = 0;
+        if (e < total) {
+            const int2 a = __ldg(p.arcs + ob + (e - oo));
+            dst = (unsigned)a.x;
+            nd = ou + (unsigned)a.y;
+            win = relax_arc(p, q, dst, nd);
+        }
+        l1_write(p, q, ring, win, dst, nd);
+    }
+}
+
+}  // namespace mlmq

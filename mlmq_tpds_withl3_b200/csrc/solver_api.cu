@@ -1,0 +1,537 @@
+// solver_api.cu -- host runtime of libmlmq_b200.so: device graphs, the solver
+// context (distance array + queue workspace + persistent launch), the
+// reference-compatible entry points and the one-shot host-buffer call.
+#include "device_common.cuh"
+#include "mlmq_b200.h"
+#include "mlmq_queue.cuh"
+#include "sssp_plain.h"
+#include "solver_internal.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace mlmq;
+
+namespace mlmq {
+
+int cuda_fail(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return MLMQ_OK;
+    std::fprintf(stderr, "mlmq_b200: %s: %s\n", what, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return MLMQ_ERR_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return MLMQ_ERR_NODEV;
+    return MLMQ_ERR_CUDA;
+}
+
+namespace {
+
+__global__ void interleave_kernel(const int *__restrict__ col, const int *__restrict__ w, int2 *arcs,
+                                  int64_t m) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        arcs[i] = make_int2(col[i], w[i]);
+}
+
+__global__ void fill_kernel(int *p, int64_t n, int v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+int ceil_log2(uint64_t x) {
+    int l = 0;
+    while ((1ull << l) < x) l++;
+    return l;
+}
+
+int env_int(const char *name, int dflt, bool *present) {
+    const char *s = std::getenv(name);
+    if (present) *present = s != nullptr;
+    return s ? std::atoi(s) : dflt;
+}
+
+}  // namespace
+
+int fill_device(int *p, int64_t n, int v, cudaStream_t s) {
+    if (n <= 0) return MLMQ_OK;
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    fill_kernel<<<blocks, 256, 0, s>>>(p, n, v);
+    return cuda_fail(cudaGetLastError(), "fill launch");
+}
+
+int validate_config(const mlmq_config &c) {
+    if (c.queue_type != MLMQ_L1SLF_L2DQ && c.queue_type != MLMQ_L1V_L2DQ)
+        return MLMQ_ERR_UNSUPPORTED;
+    if (c.delta < 1 || c.bucket_num < 1 || c.bucket_num > NB_MAX - 1) return MLMQ_ERR_ARG;
+    if (c.bucket_max < 1 || c.bucket_max > c.bucket_num) return MLMQ_ERR_ARG;
+    if (c.l2_batch < 1 || c.l2_batch > 32 || c.min_read < 1 || c.min_read > 32) return MLMQ_ERR_ARG;
+    if (c.large_degree < 1 || c.l1_spill < 1 || c.l1_spill > 32) return MLMQ_ERR_ARG;
+    if (c.warps_per_block < 1 || c.warps_per_block > 31 || c.work_blocks < 0) return MLMQ_ERR_ARG;
+    if (c.l2_cap_log2 != 0 && (c.l2_cap_log2 < 10 || c.l2_cap_log2 > 28)) return MLMQ_ERR_ARG;
+    if (c.l3_cap_log2 != 0 && (c.l3_cap_log2 < 10 || c.l3_cap_log2 > 30)) return MLMQ_ERR_ARG;
+    if (c.timeout_ms < 1) return MLMQ_ERR_ARG;
+    return MLMQ_OK;
+}
+
+int status_to_error(unsigned st) {
+    if (st & ST_QUEUE_FULL) return MLMQ_ERR_QUEUE_FULL;
+    if (st & ST_TIMEOUT) return MLMQ_ERR_TIMEOUT;
+    if (!(st & ST_DONE)) return MLMQ_ERR_STATE;
+    if (st & ST_RANGE) return MLMQ_ERR_RANGE;
+    return MLMQ_OK;
+}
+
+int device_sm_count(int *sms) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    if (prop.major < 10) {
+        std::fprintf(stderr, "mlmq_b200: device %d is sm_%d%d; this library is built for sm_100a\n",
+                     dev, prop.major, prop.minor);
+        return MLMQ_ERR_NODEV;
+    }
+    *sms = prop.multiProcessorCount;
+    return MLMQ_OK;
+}
+
+}  // namespace mlmq
+
+// ---------------------------------------------------------------------------
+extern "C" const char *mlmq_strerror(int code) {
+    switch (code) {
+        case MLMQ_OK: return "ok";
+        case MLMQ_ERR_CUDA: return "CUDA runtime error";
+        case MLMQ_ERR_ARG: return "invalid argument";
+        case MLMQ_ERR_TIMEOUT: return "device wait exceeded its time limit";
+        case MLMQ_ERR_QUEUE_FULL: return "queue ring stayed full past its time limit";
+        case MLMQ_ERR_STATE: return "call out of order or solve did not finish";
+        case MLMQ_ERR_NOMEM: return "out of memory";
+        case MLMQ_ERR_UNSUPPORTED: return "unsupported configuration";
+        case MLMQ_ERR_RANGE: return "a distance sum reached INT_MAX";
+        case MLMQ_ERR_IO: return "I/O or file format error";
+        case MLMQ_ERR_NODEV: return "no sm_100 CUDA device";
+        case MLMQ_ERR_BUSY: return "no free slot or device memory";
+        case MLMQ_ERR_MISMATCH: return "distances differ from the caller's reference";
+        default: return "unknown error";
+    }
+}
+
+extern "C" int mlmq_config_default(mlmq_config *cfg) {
+    if (!cfg) return MLMQ_ERR_ARG;
+    std::memset(cfg, 0, sizeof(*cfg));
+    // core/include/common.h:24-34, SS/SSSP/sssp.cuh:20, sssp_run.cu:895-896.
+    cfg->queue_type = MLMQ_L1SLF_L2DQ;
+    cfg->delta = 200000;
+    cfg->work_blocks = 0;
+    cfg->warps_per_block = 16;
+    cfg->l2_batch = 8;
+    cfg->bucket_num = 16;
+    cfg->bucket_max = 4;
+    cfg->min_read = 8;
+    cfg->large_degree = 16;
+    cfg->l1_spill = 32;
+    cfg->l2_cap_log2 = 0;
+    cfg->l3_cap_log2 = 0;
+    cfg->timeout_ms = 20000;
+    int rc = MLMQ_OK;
+    bool have = false;
+    int d = env_int("BENCH_DELTA", 200000, &have);
+    if (have) {
+        if (d <= 0) rc = MLMQ_ERR_ARG;
+        else cfg->delta = d;
+    }
+    int wb = env_int("MLMQ_WORK_BLOCKS", 0, &have);
+    if (have) {
+        if (wb < 1) rc = MLMQ_ERR_ARG;
+        else cfg->work_blocks = wb;
+    }
+    if (const char *qn = std::getenv("BENCH_QUEUE")) {
+        if (std::strcmp(qn, "L1SLF_L2DQ") == 0) cfg->queue_type = MLMQ_L1SLF_L2DQ;
+        else if (std::strcmp(qn, "L1V_L2DQ") == 0) cfg->queue_type = MLMQ_L1V_L2DQ;
+        else rc = MLMQ_ERR_UNSUPPORTED;
+    }
+    return rc;
+}
+
+// ---- device graphs -----------------------------------------------------------
+
+extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
+                                      const int *d_w, mlmq_graph **out) {
+    if (!out || n <= 0 || m < 0 || m >= INT_MAX || !d_row || (m > 0 && (!d_col || !d_w)))
+        return MLMQ_ERR_ARG;
+    auto *g = new (std::nothrow) mlmq_graph;
+    if (!g) return MLMQ_ERR_NOMEM;
+    g->n = n;
+    g->m = m;
+    g->d_row = const_cast<int *>(d_row);
+    g->own_row = false;
+    g->d_arcs = nullptr;
+    int rc = cuda_fail(cudaGetDevice(&g->device), "cudaGetDevice");
+    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1)),
+                            "cudaMalloc(arcs)");
+    if (!rc && m > 0) {
+        int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
+        interleave_kernel<<<blocks, 256>>>(d_col, d_w, g->d_arcs, m);
+        rc = cuda_fail(cudaGetLastError(), "interleave launch");
+        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "interleave");
+    }
+    if (rc) {
+        mlmq_graph_free(g);
+        return rc;
+    }
+    *out = g;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
+                                 mlmq_graph **out) {
+    if (!out || n <= 0 || m < 0 || m >= INT_MAX || !row || (m > 0 && (!col || !w)))
+        return MLMQ_ERR_ARG;
+    if (row[0] != 0 || row[n] != m) return MLMQ_ERR_ARG;
+    int *d_row = nullptr, *d_col = nullptr, *d_w = nullptr;
+    int rc = cuda_fail(cudaMalloc(&d_row, sizeof(int) * ((size_t)n + 1)), "cudaMalloc(row)");
+    if (!rc && m > 0) rc = cuda_fail(cudaMalloc(&d_col, sizeof(int) * (size_t)m), "cudaMalloc(col)");
+    if (!rc && m > 0) rc = cuda_fail(cudaMalloc(&d_w, sizeof(int) * (size_t)m), "cudaMalloc(w)");
+    if (!rc) rc = cuda_fail(cudaMemcpy(d_row, row, sizeof(int) * ((size_t)n + 1),
+                                       cudaMemcpyHostToDevice), "H2D row");
+    if (!rc && m > 0)
+        rc = cuda_fail(cudaMemcpy(d_col, col, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
+                       "H2D col");
+    if (!rc && m > 0)
+        rc = cuda_fail(cudaMemcpy(d_w, w, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
+                       "H2D w");
+    mlmq_graph *g = nullptr;
+    if (!rc) rc = mlmq_graph_wrap_device(n, m, d_row, d_col, d_w, &g);
+    if (d_col) cudaFree(d_col);
+    if (d_w) cudaFree(d_w);
+    if (rc) {
+        if (d_row) cudaFree(d_row);
+        return rc;
+    }
+    g->own_row = true;
+    *out = g;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m) {
+    if (!g) return MLMQ_ERR_ARG;
+    if (n) *n = g->n;
+    if (m) *m = g->m;
+    return MLMQ_OK;
+}
+
+extern "C" void mlmq_graph_free(mlmq_graph *g) {
+    if (!g) return;
+    if (g->d_arcs) cudaFree(g->d_arcs);
+    if (g->own_row && g->d_row) cudaFree(g->d_row);
+    delete g;
+}
+
+// ---- solver context ----------------------------------------------------------
+
+extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in,
+                                  mlmq_solver **out) {
+    if (!g || !out) return MLMQ_ERR_ARG;
+    mlmq_config cfg;
+    int rc = MLMQ_OK;
+    if (cfg_in) cfg = *cfg_in;
+    else if ((rc = mlmq_config_default(&cfg))) return rc;
+    if ((rc = validate_config(cfg))) return rc;
+    int sms = 0;
+    if ((rc = device_sm_count(&sms))) return rc;
+
+    auto *s = new (std::nothrow) mlmq_solver;
+    if (!s) return MLMQ_ERR_NOMEM;
+    s->g = g;
+    s->cfg = cfg;
+    s->device = g->device;
+    const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
+    s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : std::min(24, std::max(16, ceil_log2(m / 2 + 1)));
+    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : std::min(27, std::max(18, ceil_log2(2 * m)));
+    s->workers = cfg.warps_per_block;
+    int bps = 0;
+    rc = cuda_fail(plain_max_blocks_per_sm(s->workers, &bps), "occupancy");
+    if (!rc && bps < 1) rc = MLMQ_ERR_UNSUPPORTED;
+    if (!rc) {
+        const int maxgrid = bps * sms;
+        s->grid = cfg.work_blocks > 0 ? std::min(cfg.work_blocks, maxgrid) : sms;
+        if (s->grid > maxgrid) s->grid = maxgrid;
+    }
+    const size_t l2_bytes = sizeof(unsigned long long) * ((size_t)(cfg.bucket_num + 1) << s->l2_log);
+    const size_t l3_bytes = sizeof(unsigned long long) * ((size_t)1 << s->l3_log);
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming), "event");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_dist, sizeof(int) * (size_t)g->n), "cudaMalloc(dist)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l2, l2_bytes), "cudaMalloc(L2)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3, l3_bytes), "cudaMalloc(L3)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS), "cudaMalloc(ctl)");
+    if (!rc) rc = cuda_fail(cudaMallocHost(&s->h_ctl, sizeof(unsigned) * ctl::WORDS), "pinned ctl");
+    if (!rc) rc = fill_device(s->d_dist, g->n, INT_MAX, s->stream);
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(s->stream), "solver init");
+    if (rc) {
+        mlmq_solver_destroy(s);
+        return rc;
+    }
+    s->dirty = true;
+    *out = s;
+    return MLMQ_OK;
+}
+
+namespace mlmq {
+
+// Makes the queue workspace clean: every ring slot empty, every counter 0.
+static int reset_workspace(mlmq_solver *s, cudaStream_t st) {
+    const size_t l2_bytes =
+        sizeof(unsigned long long) * ((size_t)(s->cfg.bucket_num + 1) << s->l2_log);
+    const size_t l3_bytes = sizeof(unsigned long long) * ((size_t)1 << s->l3_log);
+    int rc = cuda_fail(cudaMemsetAsync(s->d_l2, 0xff, l2_bytes, st), "reset L2");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(s->d_l3, 0xff, l3_bytes, st), "reset L3");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(s->d_ctl, 0, sizeof(unsigned) * ctl::WORDS, st), "reset ctl");
+    if (!rc) s->dirty = false;
+    return rc;
+}
+
+}  // namespace mlmq
+
+extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
+    if (!s) return MLMQ_ERR_ARG;
+    if (src < 0 || src >= s->g->n) return MLMQ_ERR_ARG;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    int rc = MLMQ_OK;
+    if (s->dirty && (rc = reset_workspace(s, st))) return rc;
+    PlainParams p;
+    p.n = s->g->n;
+    p.row = s->g->d_row;
+    p.arcs = s->g->d_arcs;
+    p.dist = s->d_dist;
+    p.src = src;
+    p.l2 = s->d_l2;
+    p.l3 = s->d_l3;
+    p.ctlw = s->d_ctl;
+    p.nb = s->cfg.bucket_num;
+    p.bm = s->cfg.bucket_max;
+    p.batch = s->cfg.l2_batch;
+    p.min_read = s->cfg.min_read;
+    p.large = s->cfg.large_degree;
+    p.l1_spill = s->cfg.l1_spill;
+    p.l1_vector = s->cfg.queue_type == MLMQ_L1V_L2DQ;
+    p.delta = (unsigned)s->cfg.delta;
+    p.l2_log = s->l2_log;
+    p.l3_log = s->l3_log;
+    p.workers = s->workers;
+    p.timeout_ns = (unsigned long long)s->cfg.timeout_ms * 1000000ull;
+    rc = cuda_fail(plain_launch(p, s->grid, st), "persistent launch");
+    if (rc) {
+        s->dirty = true;
+        return rc;
+    }
+    rc = cuda_fail(cudaMemcpyAsync(s->h_ctl, s->d_ctl, sizeof(unsigned) * ctl::WORDS,
+                                   cudaMemcpyDeviceToHost, st), "status copy");
+    if (!rc) rc = cuda_fail(cudaEventRecord(s->done, st), "event record");
+    s->launched = !rc;
+    if (rc) s->dirty = true;
+    return rc;
+}
+
+extern "C" int mlmq_solver_wait(mlmq_solver *s) {
+    if (!s) return MLMQ_ERR_ARG;
+    if (!s->launched) return MLMQ_ERR_STATE;
+    int rc = cuda_fail(cudaEventSynchronize(s->done), "solve");
+    s->launched = false;
+    if (rc) {
+        s->dirty = true;
+        return rc;
+    }
+    const unsigned st = s->h_ctl[ctl::STATUS];
+    rc = status_to_error(st);
+    if (rc && rc != MLMQ_ERR_RANGE) s->dirty = true;
+    return rc;
+}
+
+extern "C" int mlmq_solver_solve(mlmq_solver *s, int src) {
+    int rc = mlmq_solver_launch(s, src, nullptr);
+    return rc ? rc : mlmq_solver_wait(s);
+}
+
+extern "C" int mlmq_solver_dist(mlmq_solver *s, int **d_dist) {
+    if (!s || !d_dist) return MLMQ_ERR_ARG;
+    *d_dist = s->d_dist;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_solver_copy_dist(mlmq_solver *s, int *h_dist) {
+    if (!s || !h_dist) return MLMQ_ERR_ARG;
+    int rc = cuda_fail(cudaMemcpyAsync(h_dist, s->d_dist, sizeof(int) * (size_t)s->g->n,
+                                       cudaMemcpyDeviceToHost, s->stream), "D2H dist");
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(s->stream), "D2H dist sync");
+    return rc;
+}
+
+extern "C" int mlmq_solver_stats(mlmq_solver *s, mlmq_solve_stats *st) {
+    if (!s || !st) return MLMQ_ERR_ARG;
+    const unsigned long long *c = reinterpret_cast<const unsigned long long *>(s->h_ctl + ctl::STATS);
+    st->pushed = c[ctl::ST_PUSHED];
+    st->l3_pushed = c[ctl::ST_L3_PUSHED];
+    st->relaxed = c[ctl::ST_RELAXED];
+    st->improved = c[ctl::ST_IMPROVED];
+    st->first_max = (uint32_t)c[ctl::ST_FIRST_MAX];
+    st->grid = s->grid;
+    st->block = 32 * (s->workers + 1);
+    st->status = s->h_ctl[ctl::STATUS];
+    return MLMQ_OK;
+}
+
+extern "C" void mlmq_solver_destroy(mlmq_solver *s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->d_dist) cudaFree(s->d_dist);
+    if (s->d_l2) cudaFree(s->d_l2);
+    if (s->d_l3) cudaFree(s->d_l3);
+    if (s->d_ctl) cudaFree(s->d_ctl);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    if (s->done) cudaEventDestroy(s->done);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+extern "C" int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
+                               int nsrc, const int *srcs, int *h_dist, const mlmq_config *cfg) {
+    if (nsrc < 0 || (nsrc > 0 && (!srcs || !h_dist))) return MLMQ_ERR_ARG;
+    mlmq_graph *g = nullptr;
+    int rc = mlmq_graph_upload(n, m, row, col, w, &g);
+    if (rc) return rc;
+    mlmq_solver *s = nullptr;
+    rc = mlmq_solver_create(g, cfg, &s);
+    for (int k = 0; !rc && k < nsrc; k++) {
+        rc = mlmq_solver_solve(s, srcs[k]);
+        if (!rc) rc = mlmq_solver_copy_dist(s, h_dist + (size_t)k * (size_t)n);
+    }
+    mlmq_solver_destroy(s);
+    mlmq_graph_free(g);
+    return rc;
+}
+
+// ---- reference entry points ---------------------------------------------------
+// Reference semantics (SS/SSSP/sssp_run.cu): one global, non-reentrant solver
+// bound to a caller-owned device CSR.
+
+// The reference's CLI (SS/SSSP/main.cu:19) defines this array of CPU-oracle
+// distances; when the library is linked into that program the BENCH lines
+// report correct=0/1 against it, as sssp_run.cu:849-853 does.
+extern int *node_data_base __attribute__((weak));
+
+namespace {
+std::mutex g_mu;
+mlmq_graph *g_graph = nullptr;
+mlmq_solver *g_solver = nullptr;
+
+double wall_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+}  // namespace
+
+namespace mlmq {
+
+int dropin_init(int m, int nnz, int *RowPtr, int *ColIdx, int *edge_data) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_solver) mlmq_solver_destroy(g_solver);
+    if (g_graph) mlmq_graph_free(g_graph);
+    g_solver = nullptr;
+    g_graph = nullptr;
+    int rc = mlmq_graph_wrap_device(m, nnz, RowPtr, ColIdx, edge_data, &g_graph);
+    mlmq_config cfg;
+    int crc = mlmq_config_default(&cfg);
+    if (!rc && crc == MLMQ_ERR_UNSUPPORTED) rc = crc;
+    if (!rc) rc = mlmq_solver_create(g_graph, &cfg, &g_solver);
+    return rc;
+}
+
+int dropin_re_init() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_solver) return MLMQ_ERR_STATE;
+    int rc = fill_device(g_solver->d_dist, g_solver->g->n, INT_MAX, g_solver->stream);
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(g_solver->stream), "re_init");
+    return rc;
+}
+
+int dropin_run(int src) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_solver) return MLMQ_ERR_STATE;
+    mlmq_config cfg;
+    int rc = mlmq_config_default(&cfg);
+    if (rc) return rc;
+    if (std::memcmp(&cfg, &g_solver->cfg, sizeof(cfg)) != 0) {
+        mlmq_solver *ns = nullptr;
+        if ((rc = mlmq_solver_create(g_graph, &cfg, &ns))) return rc;
+        mlmq_solver_destroy(g_solver);
+        g_solver = ns;
+    }
+    if (src < 0 || src >= g_graph->n) return MLMQ_ERR_ARG;
+    const char *qname = cfg.queue_type == MLMQ_L1V_L2DQ ? "L1V_L2DQ" : "L1SLF_L2DQ";
+    std::printf("MLMQ_B200_CONFIG workers=%d blocks=%d delta=%d queue=%s\n",
+                32 * g_solver->workers, g_solver->grid, cfg.delta, qname);
+    const int warmups = env_int("BENCH_WARMUPS", 2, nullptr);
+    const int repeats = env_int("BENCH_REPEATS", 3, nullptr);
+    if (warmups < 0 || repeats < 1) return MLMQ_ERR_ARG;
+    const int n = g_graph->n;
+    std::vector<int> actual;
+    int result = MLMQ_OK;
+    for (int r = 0; r < warmups + repeats; r++) {
+        const double q0 = wall_ms();
+        const double s0 = wall_ms();
+        rc = mlmq_solver_solve(g_solver, src);
+        const double s1 = wall_ms();
+        if (rc) return rc;
+        int correct = -1;
+        // A weak undefined variable has address NULL: test the address first.
+        if (&node_data_base != nullptr && node_data_base != nullptr) {
+            actual.resize((size_t)n);
+            if ((rc = mlmq_solver_copy_dist(g_solver, actual.data()))) return rc;
+            correct = std::memcmp(actual.data(), node_data_base, sizeof(int) * (size_t)n) == 0;
+            if (!correct) result = MLMQ_ERR_MISMATCH;
+        }
+        const double q1 = wall_ms();
+        std::printf("BENCH algorithm=MLMQ baseline=b200_sm100a gpu_count=1 source=%d repeat=%d "
+                    "warmup=%d queue=%s solve_ms=%.6f query_wall_ms=%.6f correct=%d\n",
+                    src, r, r < warmups, qname, s1 - s0, q1 - q0, correct);
+        std::fflush(stdout);
+    }
+    return result;
+}
+
+int dropin_cp_data(int **node_data_h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!node_data_h) return MLMQ_ERR_ARG;
+    if (!g_solver) return MLMQ_ERR_STATE;
+    int *h = (int *)std::malloc(sizeof(int) * (size_t)g_graph->n);
+    if (!h) return MLMQ_ERR_NOMEM;
+    int rc = mlmq_solver_copy_dist(g_solver, h);
+    if (rc) {
+        std::free(h);
+        return rc;
+    }
+    *node_data_h = h;
+    return MLMQ_OK;
+}
+
+}  // namespace mlmq
+
+extern "C" int sssp_init(int m, int nnz, int *RowPtr, int *ColIdx, int *edge_data) {
+    return mlmq::dropin_init(m, nnz, RowPtr, ColIdx, edge_data);
+}
+extern "C" int sssp_re_init(void) { return mlmq::dropin_re_init(); }
+extern "C" int sssp_run_adaptive(int src, graph_info info) {
+    (void)info;  // the reference ignores it too (adaptive setup is off, sssp_run.cu:894)
+    return mlmq::dropin_run(src);
+}
+extern "C" int sssp_cp_data(int **node_data_h) { return mlmq::dropin_cp_data(node_data_h); }

@@ -1,0 +1,51 @@
+// solver_internal.h -- library-private definitions shared by the host runtime
+// translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "mlmq_b200.h"
+
+struct mlmq_graph {
+    int n = 0;
+    int64_t m = 0;
+    int device = 0;
+    int *d_row = nullptr;   // n + 1 row offsets (owned when own_row)
+    bool own_row = false;
+    int2 *d_arcs = nullptr; // m interleaved {dst, weight} (always owned)
+};
+
+struct mlmq_solver {
+    const mlmq_graph *g = nullptr;
+    mlmq_config cfg{};
+    int device = 0;
+    int grid = 0, workers = 0;
+    int l2_log = 0, l3_log = 0;
+    int *d_dist = nullptr;
+    unsigned long long *d_l2 = nullptr;
+    unsigned long long *d_l3 = nullptr;
+    unsigned *d_ctl = nullptr;
+    unsigned *h_ctl = nullptr;  // pinned copy of the control block after each solve
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    bool dirty = true;          // queue workspace must be reset before the next launch
+    bool launched = false;
+};
+
+namespace mlmq {
+
+int cuda_fail(cudaError_t e, const char *what);
+int fill_device(int *p, int64_t n, int v, cudaStream_t s);
+int validate_config(const mlmq_config &c);
+int status_to_error(unsigned st);
+int device_sm_count(int *sms);
+
+// Reference entry points; exported with C linkage (solver_api.cu) and with the
+// reference's C++ linkage (drop_in.cpp).
+int dropin_init(int m, int nnz, int *RowPtr, int *ColIdx, int *edge_data);
+int dropin_re_init();
+int dropin_run(int src);
+int dropin_cp_data(int **node_data_h);
+
+}  // namespace mlmq

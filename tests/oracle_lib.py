@@ -1,0 +1,109 @@
+"""Test-side access to the CPU oracle (oracle/liboracle.so) and, when it was
+built, the reference's own sssp_sequential (oracle/_ref/libref_sssp.so).
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_sssp.so")
+INT_MAX = 2**31 - 1
+
+_vp = ctypes.c_void_p
+_oracle = None
+_ref = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"{ORACLE_SO} missing: run `make -C oracle liboracle.so`")
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.oracle_sssp_i32.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp,
+                                        ctypes.POINTER(ctypes.c_longlong)]
+        lib.oracle_sssp_i64.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp,
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_longlong)]
+        lib.oracle_sssp_many.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
+                                         _vp, ctypes.c_int]
+        _oracle = lib
+    return _oracle
+
+
+def reference():
+    """The reference's compiled sssp_sequential, or None when not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_sssp_sequential.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp,
+                                            ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_longlong)]
+        _ref = lib
+    return _ref
+
+
+def _arr(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def sssp_i32(g, src):
+    """oracle_sssp_i32 -> (dist, total_work)."""
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    d = np.empty(n, np.int32)
+    work = ctypes.c_longlong()
+    rc = oracle().oracle_sssp_i32(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src),
+                                  d.ctypes.data, ctypes.byref(work))
+    if rc:
+        raise RuntimeError(f"oracle_sssp_i32 rc={rc}")
+    return d, work.value
+
+
+def sssp_i64(g, src):
+    """oracle_sssp_i64 -> (dist, reached, max_dist)."""
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    d = np.empty(n, np.int32)
+    reached = ctypes.c_int()
+    mx = ctypes.c_longlong()
+    rc = oracle().oracle_sssp_i64(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src),
+                                  d.ctypes.data, ctypes.byref(reached), ctypes.byref(mx))
+    if rc:
+        raise RuntimeError(f"oracle_sssp_i64 rc={rc}")
+    return d, reached.value, mx.value
+
+
+def sssp_many(g, sources, threads=None):
+    """Many sources on a thread pool -> (dist[nsrc, n], work[nsrc])."""
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    srcs = _arr(sources)
+    d = np.empty((len(srcs), n), np.int32)
+    work = np.empty(len(srcs), np.int64)
+    threads = threads or os.cpu_count() or 1
+    rc = oracle().oracle_sssp_many(n, row.ctypes.data, col.ctypes.data, w.ctypes.data,
+                                   len(srcs), srcs.ctypes.data, d.ctypes.data, work.ctypes.data,
+                                   int(threads))
+    if rc:
+        raise RuntimeError(f"oracle_sssp_many rc={rc}")
+    return d, work
+
+
+def ref_sequential(g, src):
+    """The reference's own sssp_sequential -> (dist, total_work)."""
+    lib = reference()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libref_sssp.so not built")
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    d = np.empty(n, np.int32)
+    work = ctypes.c_longlong()
+    rc = lib.ref_sssp_sequential(n, len(col), row.ctypes.data, col.ctypes.data, w.ctypes.data,
+                                 int(src), d.ctypes.data, ctypes.byref(work))
+    if rc:
+        raise RuntimeError(f"ref_sssp_sequential rc={rc}")
+    return d, work.value
