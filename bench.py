@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Benchmark of the plain single-source delta-stepping solve on B200.
+
+Default workload (N=1): the planar road-like kNN graph -- 6.3M points uniform
+in the unit square, 3 nearest neighbours symmetrised, w = round(1e6*d)+1 --
+with 5 seeded sources solved one at a time and delta autotuned around
+200000.  One step = those 5 solves.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mlmq|reference]
+                  [--workload c1|c2|c3] [--sources S]
+
+* value: GTEPS = sum of arcs out of reached vertices (the oracle's
+  total_work) / summed device time of the solves, CUDA events on the launch
+  stream, inputs resident in HBM, L2 flushed (256 MiB write) between solves.
+* e2e: the same metric through mlmq_solve_host() with pinned host buffers:
+  CSR upload, every solve, every distance copy back.
+* roofline: algorithmic bytes per solve 12*m_r + 12*n_r over the kernel's
+  average duration, against the measured HBM copy bandwidth.
+* cpu_baseline: the reference's own sssp_sequential (oracle/_ref) -- or the
+  oracle port when it was not built -- on the host, one thread.
+* --impl reference: the reference's CPU implementation alone, one thread per
+  source, on the same workload and metric.
+
+Multi-GPU (torchrun): replicas only -- every rank solves the same job on its
+own GPU with no collective on the data path; time is the max over ranks.
+"""
+import argparse
+import csv
+import io
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SSSP GTEPS (plain single-source delta-stepping, queries one at a time)"
+WORKLOAD_TEXT = {
+    "c1": "grid 512x512, 4-neighbour, 10% undirected edges dropped, w U{1000..100000}, "
+          "source 0, delta 200000, L1SLF_L2DQ",
+    "c2": "kNN road-like: 6.3M points U[0,1)^2, k=3 symmetrised, w=round(1e6*d)+1, "
+          "5 seeded sources one at a time, delta autotuned around 200000, L1SLF_L2DQ",
+    "c3": "R-MAT scale 22, edge factor 16, (.57,.19,.19,.05), dedup, no self-loops, "
+          "w U{1..2^20}, 5 seeded sources one at a time, delta autotuned, L1SLF_L2DQ",
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("mlmq", "reference"), default="mlmq")
+    ap.add_argument("--workload", choices=("c1", "c2", "c3"), default="c2")
+    ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    return ap.parse_args()
+
+
+def load_workload(name, limit):
+    from mlmq_tpds_withl3_b200 import workloads
+    g, srcs = workloads.WORKLOADS[name]()
+    if limit:
+        srcs = srcs[:limit]
+    return g, srcs
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """Per-launch DRAM bytes from the committed ncu summary, if captured."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.TemporaryFile(mode="w+")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 9]
+        if not rows:
+            return None
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows]
+        util = [num(r[4]) for r in rows]
+        loaded = [s for s, u in zip(sm, util) if s is not None and (u or 0) > 0] or \
+                 [s for s in sm if s is not None]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+                "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_gteps(g, srcs, threads):
+    """Times the reference's sssp_sequential (or the oracle port) on the host."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    fn = oracle_lib.ref_sequential if oracle_lib.reference() is not None else oracle_lib.sssp_i32
+    kind = "reference" if oracle_lib.reference() is not None else "port"
+
+    def one(src):
+        t0 = time.perf_counter()
+        _, work = fn(g, src)
+        return work, time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    if threads <= 1:
+        res = [one(s) for s in srcs]
+    else:
+        with ThreadPoolExecutor(threads) as ex:
+            res = list(ex.map(one, srcs))
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    busy = sum(r[1] for r in res)
+    return work, wall, busy, kind
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    g, srcs = load_workload(args.workload, args.sources)
+    threads = max(1, min(len(srcs), os.cpu_count() or 1))
+    for _ in range(args.warmup):
+        cpu_reference_gteps(g, srcs, threads)
+    work = wall = 0.0
+    kind = "reference"
+    for _ in range(args.steps):
+        w, t, _, kind = cpu_reference_gteps(g, srcs, threads)
+        work += w
+        wall += t
+    gteps = work / wall / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_TEXT[args.workload], "n": g.n, "m": g.m,
+                   "sources": srcs},
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": kind,
+                         "sample": f"{len(srcs)} sources per step, one host thread each, "
+                                   f"sssp_sequential (SS/SSSP/main.cu:47)"},
+        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_mlmq(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, autotune, default_config
+    from mlmq_tpds_withl3_b200._lib import check, lib
+
+    g, srcs = load_workload(args.workload, args.sources)
+    dg = DeviceGraph.upload(g)
+    tune_report = None
+    if args.workload == "c1" or args.no_tune:
+        cfg = default_config(delta=200000)
+    else:
+        cfg, tune_report = autotune.tune(dg, g, srcs[:2], kind=args.workload, use_cache=False)
+    solver = Solver(dg, cfg)
+
+    # Correctness and per-query work (oracle, untimed).
+    dists, works = oracle_lib.sssp_many(g, srcs, threads=min(len(srcs), os.cpu_count() or 1))
+    reached = (dists != oracle_lib.INT_MAX).sum(axis=1)
+    correct = True
+    for k, s in enumerate(srcs):
+        solver.solve(s)
+        if not np.array_equal(solver.dist(), dists[k]):
+            correct = False
+    del dists
+
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(events):
+        for s in srcs:
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.launch(s, stream.cuda_stream)
+            e1.record(stream)
+            solver.wait()
+            if events is not None:
+                events.append((e0, e1))
+
+    for _ in range(args.warmup):
+        step(None)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    events = []
+    sampler = ClockSampler(local)
+    with sampler:
+        t_wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(events)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall0
+    if pg:
+        pg.barrier()
+    per_query_ms = np.array([a.elapsed_time(b) for a, b in events])
+    total_s = per_query_ms.sum() / 1e3
+    if pg:
+        t = torch.tensor([total_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_s = float(t.item())
+    work_step = float(np.sum(works))
+    gteps = world * work_step * args.steps / total_s / 1e9
+
+    # Roofline of the persistent kernel.
+    bytes_q = 12.0 * np.asarray(works, np.float64) + 12.0 * reached.astype(np.float64)
+    launch_s = per_query_ms / 1e3
+    achieved_gbs = float(np.sum(np.tile(bytes_q, args.steps)) / np.sum(launch_s) / 1e9)
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic("sssp_plain_kernel", args.workload)
+
+    # End to end through the host-buffer API.
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        row, col, w = pin(g.row), pin(g.col), pin(g.w)
+        src_arr = np.asarray(srcs, np.int32)
+        out = torch.empty((len(srcs), g.n), dtype=torch.int32).pin_memory()
+        e2e_steps = max(1, min(args.steps, 5))
+        walls = []
+        for i in range(e2e_steps + 1):
+            t0 = time.perf_counter()
+            check(lib.mlmq_solve_host(g.n, g.m, row.data_ptr(), col.data_ptr(), w.data_ptr(),
+                                      len(srcs), src_arr.ctypes.data, out.data_ptr(), cfg),
+                  "mlmq_solve_host")
+            if i:
+                walls.append(time.perf_counter() - t0)
+        e2e_s = float(np.sum(walls))
+        if pg:
+            t = torch.tensor([e2e_s], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * work_step * len(walls) / e2e_s / 1e9, "unit": "GTEPS",
+               "h2d_bytes_per_step": int(4 * (g.n + 1) + 8 * g.m),
+               "d2h_bytes_per_step": int(4 * g.n * len(srcs)),
+               "ms_per_step": e2e_s / len(walls) * 1e3,
+               "api": "mlmq_solve_host (pinned host CSR in, distances out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        work, wall, busy, kind = cpu_reference_gteps(g, srcs, 1)
+        cpu = {"value": work / wall / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+               "sample": f"{len(srcs)} sources of the same workload, one after another, "
+                         f"{wall:.1f} s"}
+
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return 0
+    clocks = sampler.summary()
+    line = {
+        "metric": METRIC, "value": gteps, "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator; the reference's DIMACS graphs are not available)",
+        "config": {"workload": WORKLOAD_TEXT[args.workload], "n": g.n, "m": g.m,
+                   "sources": srcs, "queue": "L1SLF_L2DQ" if cfg.queue_type == 19 else "L1V_L2DQ",
+                   "delta": cfg.delta, "warps_per_block": cfg.warps_per_block,
+                   "work_blocks": solver.stats()["grid"],
+                   "l2_between_solves": "flushed (256 MiB write, outside the timed events)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "correct": bool(correct),
+        "qps": world * len(srcs) * args.steps / total_s,
+        "latency_ms": {"p50": float(np.percentile(per_query_ms, 50)),
+                       "p99": float(np.percentile(per_query_ms, 99))},
+        "work_per_step": int(work_step),
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": achieved_gbs / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": "sssp_plain_kernel",
+                     "algorithmic_bytes_per_launch": float(np.mean(bytes_q))},
+        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "gpu_launches": len(events), "wall_s_timed_region": t_wall,
+    }
+    if tune_report:
+        line["autotune"] = {"config": tune_report.get("config"),
+                            "trials": len(tune_report.get("trials", []))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_mlmq(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

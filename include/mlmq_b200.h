@@ -60,6 +60,9 @@ const char *mlmq_strerror(int code);
 #define MLMQ_L1V_L2DQ 0
 #define MLMQ_L1SLF_L2DQ 19
 
+/* Smallest queue ring (log2 slots) a configuration may ask for. */
+#define MLMQ_MIN_RING_LOG2 18
+
 typedef struct mlmq_config {
     int queue_type;      /* MLMQ_L1SLF_L2DQ (default) or MLMQ_L1V_L2DQ */
     int delta;           /* bucket width; reference BENCH_DELTA, default 200000 */
@@ -73,8 +76,10 @@ typedef struct mlmq_config {
     int large_degree;    /* warp-cooperative relaxation at this out-degree
                             (LARGEV, 16) */
     int l1_spill;        /* L1 spills to L2 when it holds more (32) */
-    int l2_cap_log2;     /* log2 slots per L2 bucket ring; 0 = sized from graph */
-    int l3_cap_log2;     /* log2 slots of the L3 ring; 0 = sized from graph */
+    int l2_cap_log2;     /* log2 slots per L2 bucket ring; 0 = sized from graph;
+                            else MLMQ_MIN_RING_LOG2..28 */
+    int l3_cap_log2;     /* log2 slots of the L3 ring; 0 = sized from graph;
+                            else MLMQ_MIN_RING_LOG2..30 */
     int timeout_ms;      /* device wait limit per solve (default 20000) */
 } mlmq_config;
 

@@ -1,0 +1,113 @@
+"""Autotuner for the queue configuration (delta, work blocks, warps per CTA).
+
+The reference picks its queue type and delta with a fixed rule on degree and
+weight statistics (core/include/adaptive.h:64-115) and disables it in the
+timed path; this tuner instead measures: it times a few candidate
+configurations on probe sources of the actual graph and keeps the fastest.
+Every candidate gives the same exact distances (ordering changes only the
+amount of work), so tuning never affects results.
+
+Results are persisted per graph class (kind, log2 n, rounded average degree
+and log2 average weight) in a JSON file, $MLMQ_TUNE_CACHE or
+~/.cache/mlmq_b200/tune.json.
+"""
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from ._lib import default_config
+from .solver import Solver
+
+
+def graph_class(hg, kind="graph"):
+    info = hg.info()
+    return (f"{kind}:n2^{int(round(math.log2(max(hg.n, 1))))}"
+            f":deg{int(round(info.avg_nnz))}:w2^{int(round(math.log2(max(info.avg_weight, 1))))}")
+
+
+def _cache_path():
+    return os.environ.get("MLMQ_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "mlmq_b200", "tune.json"))
+
+
+def load_cache():
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def store_cache(key, value):
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        cache = load_cache()
+        cache[key] = value
+        with open(path + ".tmp", "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(path + ".tmp", path)
+    except OSError:
+        pass
+
+
+def delta_candidates(hg, around=200000):
+    """Bucket widths from a few multiples of the mean weight up to `around`."""
+    avg_w = max(1.0, float(hg.info().avg_weight))
+    cands = {int(around)}
+    for k in (2, 4, 8, 16, 32, 64):
+        cands.add(max(1, int(avg_w * k)))
+    return sorted(c for c in cands if c <= 4 * around)
+
+
+def _time_solve(solver, src, reps=2):
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        solver.solve(src)
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
+         extra=None):
+    """Returns (config, report).  Candidates: delta from delta_candidates(),
+    then warps per CTA in {8, 16, 24} at the best delta."""
+    key = graph_class(hg, kind)
+    base = dict(extra or {})
+    if use_cache:
+        hit = load_cache().get(key)
+        if hit:
+            return default_config(**{**hit["config"], **base}), {"cached": key, **hit}
+    probe = list(probe_sources)[:2]
+    results = []
+
+    def measure(over):
+        s = Solver(dgraph, {**base, **over})
+        try:
+            s.solve(probe[0])  # warm-up
+            t = sum(_time_solve(s, src) for src in probe)
+        finally:
+            s.close()
+        results.append({"config": over, "seconds": t})
+        return t
+
+    best_d = min(delta_candidates(hg, around), key=lambda d: measure({"delta": d}))
+    best = {"delta": best_d}
+    best_t = min(r["seconds"] for r in results if r["config"] == best)
+    for wpb in (8, 24):
+        over = {"delta": best_d, "warps_per_block": wpb}
+        t = measure(over)
+        if t < best_t:
+            best, best_t = over, t
+    report = {"key": key, "config": best, "seconds": best_t, "trials": results}
+    if use_cache:
+        store_cache(key, {"config": best, "seconds": best_t})
+    return default_config(**{**best, **base}), report
+
+
+def median_ms(times):
+    return float(np.median(np.asarray(times))) * 1e3

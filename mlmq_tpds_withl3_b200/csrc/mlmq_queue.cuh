@@ -363,11 +363,15 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
     int beg = 0, deg = 0;
     unsigned du = 0;
     if (valid) {
+        // The three loads are independent: issue them together rather than
+        // after the stale check.
         const int cur = __ldcg(p.dist + v);
+        const int rb = __ldg(p.row + v);
+        const int re = __ldg(p.row + v + 1);
         if ((int)d <= cur) {
             du = (unsigned)cur;
-            beg = __ldg(p.row + v);
-            deg = __ldg(p.row + v + 1) - beg;
+            beg = rb;
+            deg = re - rb;
         }
     }
     q.relaxed += (unsigned)deg;

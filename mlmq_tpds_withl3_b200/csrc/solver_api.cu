@@ -72,8 +72,14 @@ int validate_config(const mlmq_config &c) {
     if (c.l2_batch < 1 || c.l2_batch > 32 || c.min_read < 1 || c.min_read > 32) return MLMQ_ERR_ARG;
     if (c.large_degree < 1 || c.l1_spill < 1 || c.l1_spill > 32) return MLMQ_ERR_ARG;
     if (c.warps_per_block < 1 || c.warps_per_block > 31 || c.work_blocks < 0) return MLMQ_ERR_ARG;
-    if (c.l2_cap_log2 != 0 && (c.l2_cap_log2 < 10 || c.l2_cap_log2 > 28)) return MLMQ_ERR_ARG;
-    if (c.l3_cap_log2 != 0 && (c.l3_cap_log2 < 10 || c.l3_cap_log2 > 30)) return MLMQ_ERR_ARG;
+    // Ring floor: pushes that passed the pressure check before a bucket's
+    // pressure bit was set (at most 32 per warp, ~76K on a full B200) plus
+    // claimed-but-unread slots must fit in the ring's free half, so a writer
+    // never meets an unread record of the previous lap in practice.
+    if (c.l2_cap_log2 != 0 && (c.l2_cap_log2 < MLMQ_MIN_RING_LOG2 || c.l2_cap_log2 > 28))
+        return MLMQ_ERR_ARG;
+    if (c.l3_cap_log2 != 0 && (c.l3_cap_log2 < MLMQ_MIN_RING_LOG2 || c.l3_cap_log2 > 30))
+        return MLMQ_ERR_ARG;
     if (c.timeout_ms < 1) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
@@ -254,8 +260,10 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     s->cfg = cfg;
     s->device = g->device;
     const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
-    s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : std::min(24, std::max(16, ceil_log2(m / 2 + 1)));
-    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : std::min(27, std::max(18, ceil_log2(2 * m)));
+    s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2
+                                : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
+    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2
+                                : std::min(27, std::max(MLMQ_MIN_RING_LOG2 + 1, ceil_log2(2 * m)));
     s->workers = cfg.warps_per_block;
     int bps = 0;
     rc = cuda_fail(plain_max_blocks_per_sm(s->workers, &bps), "occupancy");

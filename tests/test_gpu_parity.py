@@ -69,7 +69,7 @@ def test_c1_grid512_bit_exact():
     {"warps_per_block": 4, "work_blocks": 3},
     {"large_degree": 1},
     {"l1_spill": 1},
-    {"l2_cap_log2": 10, "l3_cap_log2": 12},
+    {"l2_cap_log2": 18, "l3_cap_log2": 18},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
@@ -88,15 +88,42 @@ def test_knn_and_rmat_medium():
             assert np.array_equal(s.solve(src).dist(), ref), (g.name, src)
 
 
-def test_l3_overflow_path_exact():
-    """A tiny L2 ring and a narrow bucket window force records through the L3
-    ring (far records and ring pressure); results stay exact."""
+def test_l3_far_records_exact():
+    """A two-bucket window of narrow buckets sends most records beyond the
+    window to the L3 ring; results stay exact and L3 is exercised."""
     g = HostGraph.rmat(14, seed=8)
     ref, _ = oracle_lib.sssp_i32(g, 0)
-    s = Solver(DeviceGraph.upload(g), {"l2_cap_log2": 10, "bucket_num": 2, "bucket_max": 1,
-                                        "delta": 5000})
+    s = Solver(DeviceGraph.upload(g), {"l2_cap_log2": 18, "bucket_num": 2, "bucket_max": 1,
+                                        "delta": 5000, "timeout_ms": 10000})
     assert np.array_equal(s.solve(0).dist(), ref)
     assert s.stats()["l3_pushed"] > 0
+
+
+def test_l2_pressure_path_exact():
+    """One bucket wide enough to hold every distance fills its ring past the
+    pressure threshold, so later pushes divert to L3; results stay exact."""
+    g = HostGraph.rmat(17, seed=9)
+    ref, _ = oracle_lib.sssp_i32(g, 1)
+    s = Solver(DeviceGraph.upload(g), {"l2_cap_log2": 18, "bucket_num": 1, "bucket_max": 1,
+                                        "delta": 1 << 30, "l1_spill": 1,
+                                        "timeout_ms": 10000})
+    assert np.array_equal(s.solve(1).dist(), ref)
+
+
+def test_timeout_is_reported_not_hung():
+    """A 1 ms device time limit on a graph that needs longer ends the solve
+    with MLMQ_ERR_TIMEOUT; the next solve with a normal limit is exact."""
+    from mlmq_tpds_withl3_b200 import MlmqError
+    from mlmq_tpds_withl3_b200._lib import MLMQ_ERR_TIMEOUT
+    g = HostGraph.grid(512, 512, seed=1)
+    dg = DeviceGraph.upload(g)
+    s = Solver(dg, {"timeout_ms": 1, "delta": 1000})
+    with pytest.raises(MlmqError) as ei:
+        s.solve(0)
+    assert ei.value.code == MLMQ_ERR_TIMEOUT
+    s.close()
+    ref, _ = oracle_lib.sssp_i32(g, 0)
+    assert np.array_equal(Solver(dg).solve(0).dist(), ref)
 
 
 def test_dropin_entry_points_with_device_csr():
