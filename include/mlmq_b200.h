@@ -200,6 +200,37 @@ void mlmq_solver_destroy(mlmq_solver *s);
 int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
                     int nsrc, const int *srcs, int *h_dist, const mlmq_config *cfg);
 
+/* ---- 2c. single-source solve that allocates nothing ----------------------
+ * No counterpart in the reference: the reference solver allocates its queue
+ * storage with cudaMalloc on every run (sssp_run.cu:777-778).
+ *
+ * For callers that must not allocate device memory while they solve: code
+ * whose device memory is owned by a framework's pool allocator, a process
+ * that reserved all device memory up front, or a real-time path where an
+ * allocation could block or fail.  The queue workspace is a fixed array in
+ * the library's device image (MLMQ_NOALLOC_WORKSPACE_BYTES, about 26 MiB),
+ * held on each device from the time the library's device code is loaded
+ * there (at the latest, the first call) until the process exits.  The
+ * caller passes the device CSR (d_row[n+1], d_col[m], d_w[m], read in
+ * place) and the output d_dist[n]; nothing else is allocated.
+ *
+ *  - Graphs above MLMQ_NOALLOC_MAX_VERTICES vertices or MLMQ_NOALLOC_MAX_ARCS
+ *    arcs, and bucket_num > 16, return MLMQ_ERR_RANGE before any work; at
+ *    most 8 worker warps per CTA are used.
+ *  - cfg may be NULL (mlmq_config_default).  The call runs on `stream`
+ *    (a cudaStream_t, NULL = legacy default stream) and returns when the
+ *    solve has finished, with its status.
+ *  - The first call on a device looks up the workspace address and clears
+ *    it; make that first call before any stream capture on that device.
+ *  - All calls share the one workspace and it keeps the last call's
+ *    contents: calls whose kernels overlap on the GPU (two host threads,
+ *    two streams) race and corrupt each other's results.  Serialise them. */
+#define MLMQ_NOALLOC_MAX_VERTICES (1 << 20)
+#define MLMQ_NOALLOC_MAX_ARCS (1 << 20)
+#define MLMQ_NOALLOC_WORKSPACE_BYTES 26215744
+int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int *d_col, const int *d_w,
+                            int src, int *d_dist, const mlmq_config *cfg, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,6 +119,11 @@ _sig("mlmq_solver_stats", c_int, c_vp, ctypes.POINTER(SolveStats))
 _sig("mlmq_solver_destroy", None, c_vp)
 _sig("mlmq_solve_host", c_int, c_int, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp,
      ctypes.POINTER(Config))
+# single-source solve that allocates nothing (fixed workspace in the library)
+_sig("mlmq_sssp_solve_noalloc", c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, c_vp,
+     ctypes.POINTER(Config), c_vp)
+NOALLOC_MAX_VERTICES = 1 << 20
+NOALLOC_MAX_ARCS = 1 << 20
 
 
 def default_config(**overrides):

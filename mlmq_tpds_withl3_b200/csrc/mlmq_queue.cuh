@@ -51,7 +51,9 @@ namespace mlmq {
 struct PlainParams {
     int n;
     const int *__restrict__ row;
-    const int2 *__restrict__ arcs;  // interleaved {dst, weight}
+    const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
+    const int *__restrict__ col;    // caller's CSR arrays, read in place (ArcsSplit)
+    const int *__restrict__ w;
     int *dist;
     int src;
     unsigned long long *l2;  // (nb + 1) rings of 2^l2_log slots; ring nb is the urgent ring
@@ -340,6 +342,20 @@ __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile 
 }
 
 // ---- relaxation --------------------------------------------------------------
+// Arc loaders.  The allocating solver builds one interleaved {dst, weight}
+// array so an arc is one 8-byte load; the no-allocation entry point cannot
+// build it and reads the caller's ColIdx and edge_data arrays in place.
+struct ArcsInterleaved {
+    static __device__ __forceinline__ int2 load(const PlainParams &p, int i) {
+        return __ldg(p.arcs + i);
+    }
+};
+struct ArcsSplit {
+    static __device__ __forceinline__ int2 load(const PlainParams &p, int i) {
+        return make_int2(__ldg(p.col + i), __ldg(p.w + i));
+    }
+};
+
 __device__ __forceinline__ bool relax_arc(const PlainParams &p, WarpQ &q, unsigned dst,
                                           unsigned nd) {
     const int cur = __ldcg(p.dist + dst);
@@ -357,6 +373,7 @@ __device__ __forceinline__ bool relax_arc(const PlainParams &p, WarpQ &q, unsign
 }
 
 // Relaxes up to 32 records (one per lane) and feeds the winners to L1.
+template <class Arcs>
 __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
                                             unsigned v, unsigned d) {
     const int lane = threadIdx.x & 31;
@@ -388,7 +405,7 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
             bool win = false;
             unsigned dst = 0, nd = 0;
             if (e < ld) {
-                const int2 a = __ldg(p.arcs + lb + e);
+                const int2 a = Arcs::load(p, lb + e);
                 dst = (unsigned)a.x;
                 nd = lu + (unsigned)a.y;
                 win = relax_arc(p, q, dst, nd);
@@ -422,7 +439,7 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         bool win = false;
         unsigned dst = 0, nd = 0;
         if (e < total) {
-            const int2 a = __ldg(p.arcs + ob + (e - oo));
+            const int2 a = Arcs::load(p, ob + (e - oo));
             dst = (unsigned)a.x;
             nd = ou + (unsigned)a.y;
             win = relax_arc(p, q, dst, nd);

@@ -319,6 +319,8 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.n = s->g->n;
     p.row = s->g->d_row;
     p.arcs = s->g->d_arcs;
+    p.col = nullptr;
+    p.w = nullptr;
     p.dist = s->d_dist;
     p.src = src;
     p.l2 = s->d_l2;

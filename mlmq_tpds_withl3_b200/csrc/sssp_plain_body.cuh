@@ -1,0 +1,221 @@
+// sssp_plain_body.cuh -- body of the persistent single-source kernel, shared by
+// the allocating solver (sssp_plain.cu) and the no-allocation entry point
+// (noalloc.cu).  `Arcs` selects how arcs are read (see mlmq_queue.cuh).
+//
+// One cooperative launch per query (reference: work_block_kernel +
+// manage_block_kernel on two streams, SS/SSSP/sssp_run.cu:415-674, whose
+// manager only ran if the GPU happened to have a free SM).  Every CTA is
+// `workers` worker warps plus one manager warp; the cooperative launch
+// guarantees all CTAs are resident, so the in-kernel barriers and the
+// manager/worker hand-offs cannot wait on a CTA that never started.
+//
+// Prologue: fill dist with INT_MAX, reset the queue counters, barrier, seed
+// the source record into bucket 0, barrier.  Then workers loop
+// L1 -> L2 window -> L3 -> relax, and manager warps mirror the counters into
+// shared memory; CTA 0's manager also detects termination and moves `first`.
+#pragma once
+
+#include "mlmq_queue.cuh"
+
+namespace mlmq {
+
+__device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirror &mir,
+                                             unsigned long long deadline) {
+    const int lane = threadIdx.x & 31;
+    const bool controller = blockIdx.x == 0;
+    const int rings = p.nb + 1;  // buckets + urgent ring
+    const unsigned cap8 = 1u << (p.l2_log - 3);
+    unsigned ns = 64;
+    for (;;) {
+        // Credit is read (acquire) before the reserve counters: a credit is
+        // returned only after the pushes it covers, so any credit seen here
+        // comes with its reserves and the difference can only overstate the
+        // outstanding work.
+        const unsigned credit = controller ? ld_acquire(p.ctlw + ctl::CREDIT) : 0u;
+        unsigned res = 0, clm = 0, con = 0;
+        if (lane < rings) {
+            res = ld_relaxed(p.ctlw + ctl::RESERVE + lane);
+            clm = ld_relaxed(p.ctlw + ctl::CLAIM + lane);
+            con = ld_relaxed(p.ctlw + ctl::CONSUMED + lane);
+        }
+        const unsigned first = ld_relaxed(p.ctlw + ctl::FIRST);
+        const unsigned pres = ld_relaxed(p.ctlw + ctl::PRESSURE);
+        const unsigned l3r = ld_relaxed(p.ctlw + ctl::L3_RESERVE);
+        const unsigned l3c = ld_relaxed(p.ctlw + ctl::L3_CLAIM);
+        const unsigned l3k = ld_relaxed(p.ctlw + ctl::L3_CONSUMED);
+        unsigned ex = ld_relaxed(p.ctlw + ctl::EXIT);
+        if (lane < rings) {
+            mir.reserve[lane] = res;
+            mir.claim[lane] = clm;
+            mir.consumed[lane] = con;
+        }
+        if (lane == 0) {
+            mir.first = first;
+            mir.pressure = pres;
+            mir.l3_reserve = l3r;
+            mir.l3_claim = l3c;
+            mir.l3_consumed = l3k;
+        }
+        if (controller && !ex) {
+            unsigned sum = lane < rings ? res : 0u;
+            unsigned wait = lane < p.nb ? res - con : 0u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sum += __shfl_xor_sync(FULL, sum, o);
+                wait += __shfl_xor_sync(FULL, wait, o);
+            }
+            if (sum + l3r == credit) {
+                if (lane == 0) {
+                    atomicOr(p.ctlw + ctl::STATUS, ST_DONE);
+                    st_release(p.ctlw + ctl::EXIT, 1u);
+                }
+                ex = 1;
+            } else {
+                if (wait != 0) {
+                    // Move `first` to the first non-empty bucket of the window.
+                    const int b = (int)((first + (unsigned)lane) % (unsigned)p.nb);
+                    const unsigned rb = __shfl_sync(FULL, res, b);
+                    const unsigned cb = __shfl_sync(FULL, con, b);
+                    const unsigned ne = __ballot_sync(FULL, lane < p.nb && rb != cb);
+                    const int i0 = ne ? __ffs(ne) - 1 : 0;
+                    if (i0 > 0 && lane == 0) atomicMax(p.ctlw + ctl::FIRST, first + (unsigned)i0);
+                }
+                // Release bucket pressure once the ring has drained.
+                if (lane < p.nb && ((pres >> lane) & 1u) && res - con < cap8)
+                    atomicAnd(p.ctlw + ctl::PRESSURE, ~(1u << lane));
+            }
+        }
+        if (!ex && globaltimer() > deadline) {
+            if (lane == 0) raise_status(p, ST_TIMEOUT);
+            ex = 1;
+        }
+        ex = __shfl_sync(FULL, ex, 0);
+        if (ex) {
+            if (lane == 0) mir.exit = 1;
+            return;
+        }
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+    }
+}
+
+template <class Arcs>
+__device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirror &mir, uint2 *ring,
+                                            uint2 *inb, WarpQ &q) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        if (mir.exit) break;
+        bool valid = false;
+        unsigned v = 0, d = 0;
+        if (q.l1_size > 0) {
+            l1_read(q, ring, valid, v, d);
+        } else {
+            if (q.onfly) {
+                // L1 is empty: everything derived from the records read so far
+                // is reserved in L2/L3, so their credit may go back.
+                __threadfence();
+                __syncwarp();
+                if (lane == 0) atomicAdd(p.ctlw + ctl::CREDIT, q.onfly);
+                q.onfly = 0;
+            }
+            int got = l2_read(p, q, mir, inb);
+            if (got == 0) got = l3_read(p, q, mir, inb);
+            if (got == 0) {
+                __nanosleep(q.idle_ns);
+                if (q.idle_ns < 256) q.idle_ns <<= 1;
+                continue;
+            }
+            q.idle_ns = 32;
+            q.onfly += (unsigned)got;
+            __syncwarp();
+            valid = lane < got;
+            if (valid) {
+                const uint2 it = inb[lane];
+                v = it.x;
+                d = it.y;
+            }
+            __syncwarp();
+        }
+        relax_batch<Arcs>(p, q, ring, valid, v, d);
+    }
+}
+
+template <class Arcs>
+__device__ __forceinline__ void plain_body(const PlainParams &p) {
+    extern __shared__ uint2 smem[];
+    __shared__ Mirror mir_storage;
+    volatile Mirror &mir = mir_storage;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long deadline = globaltimer() + p.timeout_ns;
+
+    // ---- prologue: reset ------------------------------------------------------
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t gstride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = gtid; i < (size_t)p.n; i += gstride) p.dist[i] = INT_MAX;
+    if (blockIdx.x == 0) {
+        for (int i = threadIdx.x; i < ctl::WORDS; i += blockDim.x)
+            if (i != ctl::BAR_COUNT && i != ctl::BAR_GEN) p.ctlw[i] = 0u;
+    }
+    if (!grid_barrier(p.ctlw, gridDim.x, deadline)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        p.dist[p.src] = 0;
+        *l2_slot(p, 0, 0u) = rec_pack((unsigned)p.src, 0u, 0u);
+        p.ctlw[ctl::RESERVE + 0] = 1u;
+        p.ctlw[ctl::STATS + 2 * ctl::ST_PUSHED] = 1u;
+    }
+    if (!grid_barrier(p.ctlw, gridDim.x, deadline)) return;
+
+    // ---- initial mirror ----------------------------------------------------------
+    if (threadIdx.x < NB_MAX) {
+        mir.reserve[threadIdx.x] = ld_relaxed(p.ctlw + ctl::RESERVE + threadIdx.x);
+        mir.claim[threadIdx.x] = 0u;
+        mir.consumed[threadIdx.x] = 0u;
+    }
+    if (threadIdx.x == 0) {
+        mir.first = 0u;
+        mir.exit = 0u;
+        mir.pressure = 0u;
+        mir.l3_reserve = mir.l3_claim = mir.l3_consumed = 0u;
+    }
+    __syncthreads();
+
+    if (warp == p.workers) {
+        manager_loop(p, mir, deadline);
+        return;
+    }
+
+    uint2 *ring = smem + (size_t)warp * (L1_CAP + 32);
+    uint2 *inb = ring + L1_CAP;
+    WarpQ q;
+    q.l1_head = q.l1_tail = q.l1_size = 0;
+    q.c_lo = q.c_hi = 0u;
+    q.l3_lo = q.l3_hi = 0u;
+    q.onfly = 0u;
+    q.idle_ns = 32u;
+    q.range_hit = 0u;
+    q.pushed = q.l3_pushed = q.relaxed = q.improved = 0ull;
+    q.deadline = deadline;
+
+    worker_loop<Arcs>(p, mir, ring, inb, q);
+
+    // ---- epilogue: statistics --------------------------------------------------
+    unsigned long long relaxed = q.relaxed, improved = q.improved;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        relaxed += __shfl_xor_sync(FULL, relaxed, o);
+        improved += __shfl_xor_sync(FULL, improved, o);
+    }
+    const unsigned range = __ballot_sync(FULL, q.range_hit != 0u);
+    if (lane == 0) {
+        unsigned long long *st = reinterpret_cast<unsigned long long *>(p.ctlw + ctl::STATS);
+        atomicAdd(st + ctl::ST_PUSHED, q.pushed);
+        atomicAdd(st + ctl::ST_L3_PUSHED, q.l3_pushed);
+        atomicAdd(st + ctl::ST_RELAXED, relaxed);
+        atomicAdd(st + ctl::ST_IMPROVED, improved);
+        if (range) atomicOr(p.ctlw + ctl::STATUS, ST_RANGE);
+        atomicMax(st + ctl::ST_FIRST_MAX, (unsigned long long)ld_relaxed(p.ctlw + ctl::FIRST));
+    }
+}
+
+}  // namespace mlmq
