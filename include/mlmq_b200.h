@@ -200,7 +200,58 @@ void mlmq_solver_destroy(mlmq_solver *s);
 int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
                     int nsrc, const int *srcs, int *h_dist, const mlmq_config *cfg);
 
-/* ---- 2c. single-source solve that allocates nothing ----------------------
+/* ---- 2c. batched multi-source solve ---------------------------------------
+ * Many queries -- sources on one graph, or on several graphs of uneven size
+ * -- in ONE persistent launch.  Replaces the reference's back-to-back solver
+ * runs per source (SSSP/main.cu:213-307).  Each query slot owns a distance
+ * array of max_vertices entries and its own queue rings; the CTAs of the
+ * launch are split into one contiguous group per slot. */
+typedef struct mlmq_batch mlmq_batch;
+/* cfg may be NULL: mlmq_config_default() with 8 worker warps per CTA.
+ * Per-slot rings default to 2^18 slots (L2) and 2^20 slots (L3). */
+int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_config *cfg,
+                      mlmq_batch **out);
+int mlmq_batch_info(const mlmq_batch *b, int *grid, int *block, int *max_queries);
+/* Enqueues one launch solving query q from srcs[q] on graphs[q], q < nq.
+ * use_graph != 0: the launch (parameter upload, kernel, status download) is
+ * captured in a CUDA graph the first time a query set is seen and replayed
+ * while the set is unchanged. */
+int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *graphs, const int *srcs,
+                   int use_graph, void *stream);
+/* Blocks until the launch ends; the first failing query's MLMQ_ERR_* code. */
+int mlmq_batch_wait(mlmq_batch *b);
+int mlmq_batch_query_status(const mlmq_batch *b, int q, unsigned *status,
+                            mlmq_solve_stats *st);
+int mlmq_batch_dist(mlmq_batch *b, int q, int **d_dist);
+int mlmq_batch_copy_dist(mlmq_batch *b, int q, int *h_dist);
+void mlmq_batch_destroy(mlmq_batch *b);
+
+/* ---- 2d. continuous-batching server ---------------------------------------
+ * No counterpart in the reference (its only multi-query form is the
+ * back-to-back batch above).  One persistent launch serves single-source
+ * queries on HBM-resident device graphs as they arrive: the grid is split
+ * into `slots` CTA groups; a submitted query goes to a free slot, its work
+ * overlaps the other slots' queries on the device, and its distances are
+ * copied to the caller's host buffer when it finishes.  Slots are admitted
+ * by free device memory: at creation the server takes as many of the
+ * requested slots as fit in free memory minus a 2 GiB reserve.  The launch
+ * ends after lifetime_ms or mlmq_server_stop. */
+typedef struct mlmq_server mlmq_server;
+int mlmq_server_create(int slots, int max_vertices, const mlmq_config *cfg, int lifetime_ms,
+                       mlmq_server **out);
+int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block);
+/* Non-blocking.  MLMQ_ERR_BUSY when every slot is taken; h_out (n ints) must
+ * stay valid until the ticket is reported by mlmq_server_poll. */
+int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
+                       uint64_t *ticket);
+/* Advances finished queries (result copy-out) and reports up to `max`
+ * completed tickets with their MLMQ_ERR_* status. */
+int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max, int *count);
+int mlmq_server_busy_slots(mlmq_server *sv, int *busy);
+int mlmq_server_stop(mlmq_server *sv);
+void mlmq_server_destroy(mlmq_server *sv);
+
+/* ---- 2e. single-source solve that allocates nothing ----------------------
  * No counterpart in the reference: the reference solver allocates its queue
  * storage with cudaMalloc on every run (sssp_run.cu:777-778).
  *

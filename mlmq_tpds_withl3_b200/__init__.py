@@ -9,9 +9,10 @@ from ._lib import Config, GraphInfo, MlmqError, default_config, MLMQ_L1SLF_L2DQ,
 from .graph import HostGraph
 from .solver import (DeviceGraph, Solver, solve_host, sssp_init, sssp_re_init,
                      sssp_run_adaptive, sssp_cp_data, INT_MAX)
+from .batch import BatchSolver
 
 __all__ = [
     "Config", "GraphInfo", "MlmqError", "default_config", "MLMQ_L1SLF_L2DQ", "MLMQ_L1V_L2DQ",
     "HostGraph", "DeviceGraph", "Solver", "solve_host", "sssp_init", "sssp_re_init",
-    "sssp_run_adaptive", "sssp_cp_data", "INT_MAX",
+    "sssp_run_adaptive", "sssp_cp_data", "INT_MAX", "BatchSolver",
 ]

@@ -119,6 +119,28 @@ _sig("mlmq_solver_stats", c_int, c_vp, ctypes.POINTER(SolveStats))
 _sig("mlmq_solver_destroy", None, c_vp)
 _sig("mlmq_solve_host", c_int, c_int, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp,
      ctypes.POINTER(Config))
+# batched multi-source solve
+_sig("mlmq_batch_create", c_int, c_int, c_int, ctypes.POINTER(Config), ctypes.POINTER(c_vp))
+_sig("mlmq_batch_info", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+     ctypes.POINTER(c_int))
+_sig("mlmq_batch_run", c_int, c_vp, c_int, ctypes.POINTER(c_vp), c_vp, c_int, c_vp)
+_sig("mlmq_batch_wait", c_int, c_vp)
+_sig("mlmq_batch_query_status", c_int, c_vp, c_int, ctypes.POINTER(c_u32),
+     ctypes.POINTER(SolveStats))
+_sig("mlmq_batch_dist", c_int, c_vp, c_int, ctypes.POINTER(c_vp))
+_sig("mlmq_batch_copy_dist", c_int, c_vp, c_int, c_vp)
+_sig("mlmq_batch_destroy", None, c_vp)
+# continuous-batching server
+_sig("mlmq_server_create", c_int, c_int, c_int, ctypes.POINTER(Config), c_int,
+     ctypes.POINTER(c_vp))
+_sig("mlmq_server_info", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+     ctypes.POINTER(c_int))
+_sig("mlmq_server_submit", c_int, c_vp, c_vp, c_int, c_vp, ctypes.POINTER(c_u64))
+_sig("mlmq_server_poll", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_int), c_int,
+     ctypes.POINTER(c_int))
+_sig("mlmq_server_busy_slots", c_int, c_vp, ctypes.POINTER(c_int))
+_sig("mlmq_server_stop", c_int, c_vp)
+_sig("mlmq_server_destroy", None, c_vp)
 # single-source solve that allocates nothing (fixed workspace in the library)
 _sig("mlmq_sssp_solve_noalloc", c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, c_vp,
      ctypes.POINTER(Config), c_vp)

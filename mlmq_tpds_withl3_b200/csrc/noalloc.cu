@@ -53,7 +53,7 @@ static_assert(NA_TOTAL_U64 * 8 == MLMQ_NOALLOC_WORKSPACE_BYTES, "header constant
 static __device__ __align__(256) unsigned long long g_noalloc_ws[NA_TOTAL_U64];
 
 __global__ void __launch_bounds__(1024, 1) sssp_noalloc_kernel(PlainParams p) {
-    plain_body<ArcsSplit>(p);
+    plain_body<ArcsSplit>(p, blockIdx.x, gridDim.x);
 }
 
 struct DeviceSlot {

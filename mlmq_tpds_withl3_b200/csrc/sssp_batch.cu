@@ -1,0 +1,333 @@
+// sssp_batch.cu -- many single-source queries, on one or several graphs of
+// uneven size, solved in ONE persistent launch.
+//
+// The reference's multi-source form is back-to-back full solver runs, one per
+// source (SSSP/main.cu:213-307, run_multi_source_batch).  Here a launch hosts
+// `nq` query slots.  Slot s is served by a contiguous group of CTAs
+// (CTA c belongs to slot floor(c * nq / grid)); each slot owns its distance
+// array, its L2/L3 rings and its control block, so every slot runs the
+// single-source algorithm of sssp_plain_body.cuh unchanged -- its own
+// termination, its own `first` -- while all slots share the graph arrays.
+// A road-like query is bound by the latency of its dependent relaxations,
+// not by bandwidth; running the queries side by side fills the GPU with
+// independent chains, which is where the batched throughput comes from.
+// Queries on the same graph read the same CSR, so its lines are shared in L2.
+//
+// The launch (parameter upload, kernel, status download) can be captured in
+// a CUDA graph and replayed (mlmq_batch_run with use_graph = 1).
+#include "mlmq_b200.h"
+#include "solver_internal.h"
+#include "sssp_plain.h"
+#include "sssp_plain_body.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace mlmq {
+
+constexpr int CTL_STRIDE = 512;  // words per slot control block (2 KiB, padded)
+
+__global__ void __launch_bounds__(1024, 1) sssp_batch_kernel(const PlainParams *__restrict__ slots,
+                                                             int nq) {
+    const unsigned g = gridDim.x;
+    const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)nq) / g);
+    // First CTA of slot s: ceil(s * g / nq).
+    const unsigned lo = (unsigned)(((unsigned long long)s * g + nq - 1) / (unsigned)nq);
+    const unsigned hi = (unsigned)(((unsigned long long)(s + 1) * g + nq - 1) / (unsigned)nq);
+    const PlainParams p = slots[s];
+    plain_body<ArcsInterleaved>(p, blockIdx.x - lo, hi - lo);
+}
+
+}  // namespace mlmq
+
+using namespace mlmq;
+
+struct mlmq_batch {
+    int device = 0;
+    mlmq_config cfg{};
+    int max_q = 0, max_n = 0;
+    int grid = 0, workers = 0, l2_log = 0, l3_log = 0;
+    int *d_dist = nullptr;            // max_q * max_n
+    unsigned long long *d_l2 = nullptr;
+    unsigned long long *d_l3 = nullptr;
+    unsigned *d_ctl = nullptr;        // max_q * CTL_STRIDE
+    PlainParams *d_params = nullptr;  // max_q
+    PlainParams *h_params = nullptr;  // pinned
+    unsigned *h_ctl = nullptr;        // pinned copy of the control blocks
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    bool dirty = true, launched = false;
+    int nq = 0;
+    std::vector<int> n_of;            // vertex count per active slot
+    cudaGraphExec_t exec = nullptr;   // captured launch of the current query set
+    std::vector<long long> exec_key;  // (graph pointer, src) per slot of `exec`
+    bool graph_cooperative = true;
+};
+
+namespace {
+
+size_t l2_slots(const mlmq_batch *b) { return (size_t)(b->cfg.bucket_num + 1) << b->l2_log; }
+
+int reset_all(mlmq_batch *b, cudaStream_t st) {
+    int rc = cuda_fail(cudaMemsetAsync(b->d_l2, 0xff, sizeof(unsigned long long) * l2_slots(b) * b->max_q, st),
+                       "batch reset L2");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(b->d_l3, 0xff,
+                                            sizeof(unsigned long long) * ((size_t)b->max_q << b->l3_log), st),
+                            "batch reset L3");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(b->d_ctl, 0, sizeof(unsigned) * CTL_STRIDE * b->max_q, st),
+                            "batch reset ctl");
+    if (!rc) b->dirty = false;
+    return rc;
+}
+
+int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
+    const int threads = 32 * (b->workers + 1);
+    const size_t smem = plain_smem_bytes(b->workers);
+    int rc = cuda_fail(cudaMemcpyAsync(b->d_params, b->h_params, sizeof(PlainParams) * nq,
+                                       cudaMemcpyHostToDevice, st), "batch params");
+    if (rc) return rc;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)b->grid);
+    lc.blockDim = dim3((unsigned)threads);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    lc.attrs = attr;
+    lc.numAttrs = b->graph_cooperative ? 1 : 0;
+    const PlainParams *params = b->d_params;
+    rc = cuda_fail(cudaLaunchKernelEx(&lc, sssp_batch_kernel, params, nq), "batch launch");
+    if (rc) return rc;
+    return cuda_fail(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq,
+                                     cudaMemcpyDeviceToHost, st), "batch status");
+}
+
+}  // namespace
+
+extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_config *cfg_in,
+                                 mlmq_batch **out) {
+    if (!out || max_queries < 1 || max_vertices < 1) return MLMQ_ERR_ARG;
+    mlmq_config cfg;
+    int rc = MLMQ_OK;
+    if (cfg_in) cfg = *cfg_in;
+    else {
+        if ((rc = mlmq_config_default(&cfg))) return rc;
+        cfg.warps_per_block = 8;
+    }
+    if ((rc = validate_config(cfg))) return rc;
+    int sms = 0;
+    if ((rc = device_sm_count(&sms))) return rc;
+    auto *b = new (std::nothrow) mlmq_batch;
+    if (!b) return MLMQ_ERR_NOMEM;
+    b->cfg = cfg;
+    b->max_q = max_queries;
+    b->max_n = max_vertices;
+    b->workers = cfg.warps_per_block;
+    b->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : MLMQ_MIN_RING_LOG2;
+    b->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : MLMQ_MIN_RING_LOG2 + 2;
+    rc = cuda_fail(cudaGetDevice(&b->device), "cudaGetDevice");
+    int bps = 0;
+    if (!rc) {
+        const int threads = 32 * (b->workers + 1);
+        const size_t smem = plain_smem_bytes(b->workers);
+        rc = cuda_fail(cudaFuncSetAttribute(sssp_batch_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                       "batch smem");
+        if (!rc)
+            rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_batch_kernel,
+                                                                         threads, smem),
+                           "batch occupancy");
+    }
+    if (!rc) {
+        const int maxgrid = bps * sms;
+        b->grid = cfg.work_blocks > 0 ? std::min(cfg.work_blocks, maxgrid) : maxgrid;
+        if (b->grid < max_queries) {
+            std::fprintf(stderr, "mlmq_batch_create: %d query slots need at least one CTA each; "
+                                 "at most %d CTAs fit\n", max_queries, b->grid);
+            rc = MLMQ_ERR_RANGE;
+        }
+    }
+    const size_t nq = (size_t)max_queries;
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_dist, sizeof(int) * nq * (size_t)max_vertices), "batch dist");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l2, sizeof(unsigned long long) * l2_slots(b) * nq), "batch L2");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3, sizeof(unsigned long long) * (nq << b->l3_log)), "batch L3");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "batch ctl");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_params, sizeof(PlainParams) * nq), "batch params");
+    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_params, sizeof(PlainParams) * nq), "pinned params");
+    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "pinned ctl");
+    if (!rc) rc = reset_all(b, b->stream);
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(b->stream), "batch init");
+    if (rc) {
+        mlmq_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_batch_info(const mlmq_batch *b, int *grid, int *block, int *max_queries) {
+    if (!b) return MLMQ_ERR_ARG;
+    if (grid) *grid = b->grid;
+    if (block) *block = 32 * (b->workers + 1);
+    if (max_queries) *max_queries = b->max_q;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *graphs,
+                              const int *srcs, int use_graph, void *stream) {
+    if (!b || nq < 1 || nq > b->max_q || !graphs || !srcs) return MLMQ_ERR_ARG;
+    for (int q = 0; q < nq; q++) {
+        if (!graphs[q] || graphs[q]->n > b->max_n || srcs[q] < 0 || srcs[q] >= graphs[q]->n)
+            return MLMQ_ERR_ARG;
+        if (graphs[q]->device != b->device) return MLMQ_ERR_ARG;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    int rc = MLMQ_OK;
+    if (b->dirty && (rc = reset_all(b, st))) return rc;
+    const size_t l2s = l2_slots(b);
+    std::vector<long long> key;
+    key.reserve(2 * (size_t)nq);
+    b->n_of.assign((size_t)nq, 0);
+    for (int q = 0; q < nq; q++) {
+        const mlmq_graph *g = graphs[q];
+        PlainParams &p = b->h_params[q];
+        std::memset(&p, 0, sizeof(p));
+        p.n = g->n;
+        p.row = g->d_row;
+        p.arcs = g->d_arcs;
+        p.dist = b->d_dist + (size_t)q * b->max_n;
+        p.src = srcs[q];
+        p.l2 = b->d_l2 + (size_t)q * l2s;
+        p.l3 = b->d_l3 + ((size_t)q << b->l3_log);
+        p.ctlw = b->d_ctl + (size_t)q * CTL_STRIDE;
+        p.nb = b->cfg.bucket_num;
+        p.bm = b->cfg.bucket_max;
+        p.batch = b->cfg.l2_batch;
+        p.min_read = b->cfg.min_read;
+        p.large = b->cfg.large_degree;
+        p.l1_spill = b->cfg.l1_spill;
+        p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
+        p.delta = (unsigned)b->cfg.delta;
+        p.l2_log = b->l2_log;
+        p.l3_log = b->l3_log;
+        p.workers = b->workers;
+        p.timeout_ns = (unsigned long long)b->cfg.timeout_ms * 1000000ull;
+        b->n_of[q] = g->n;
+        key.push_back((long long)(uintptr_t)g);
+        key.push_back(srcs[q]);
+    }
+    b->nq = nq;
+    if (use_graph) {
+        // Replay the captured launch when the query set is unchanged; the
+        // parameters are read from the pinned host array at replay time.
+        if (!b->exec || b->exec_key != key) {
+            if (b->exec) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            cudaGraph_t graph = nullptr;
+            for (int attempt = 0; attempt < 2 && !b->exec; attempt++) {
+                rc = cuda_fail(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                               "begin capture");
+                if (rc) return rc;
+                int erc = enqueue(b, nq, st);
+                cudaError_t ce = cudaStreamEndCapture(st, &graph);
+                if (erc == MLMQ_OK && ce == cudaSuccess) {
+                    cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+                    if (ie != cudaSuccess) b->exec = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
+                graph = nullptr;
+                cudaGetLastError();
+                // Some drivers refuse cooperative kernels in graphs; the grid
+                // never exceeds the occupancy limit, so a plain launch keeps
+                // every CTA resident on an otherwise idle GPU.
+                if (!b->exec) b->graph_cooperative = false;
+            }
+            if (!b->exec) return cuda_fail(cudaErrorNotSupported, "graph capture");
+            b->exec_key = key;
+        }
+        rc = cuda_fail(cudaGraphLaunch(b->exec, st), "graph launch");
+    } else {
+        b->graph_cooperative = true;
+        rc = enqueue(b, nq, st);
+    }
+    if (!rc) rc = cuda_fail(cudaEventRecord(b->done, st), "batch event");
+    b->launched = !rc;
+    if (rc) b->dirty = true;
+    return rc;
+}
+
+extern "C" int mlmq_batch_wait(mlmq_batch *b) {
+    if (!b) return MLMQ_ERR_ARG;
+    if (!b->launched) return MLMQ_ERR_STATE;
+    b->launched = false;
+    int rc = cuda_fail(cudaEventSynchronize(b->done), "batch solve");
+    if (rc) {
+        b->dirty = true;
+        return rc;
+    }
+    int worst = MLMQ_OK;
+    for (int q = 0; q < b->nq; q++) {
+        const int e = status_to_error(b->h_ctl[(size_t)q * CTL_STRIDE + ctl::STATUS]);
+        if (e != MLMQ_OK && e != MLMQ_ERR_RANGE) b->dirty = true;
+        if (e != MLMQ_OK && worst == MLMQ_OK) worst = e;
+    }
+    return worst;
+}
+
+extern "C" int mlmq_batch_query_status(const mlmq_batch *b, int q, unsigned *status,
+                                       mlmq_solve_stats *st) {
+    if (!b || q < 0 || q >= b->nq) return MLMQ_ERR_ARG;
+    const unsigned *c = b->h_ctl + (size_t)q * CTL_STRIDE;
+    if (status) *status = c[ctl::STATUS];
+    if (st) {
+        const unsigned long long *u = reinterpret_cast<const unsigned long long *>(c + ctl::STATS);
+        st->pushed = u[ctl::ST_PUSHED];
+        st->l3_pushed = u[ctl::ST_L3_PUSHED];
+        st->relaxed = u[ctl::ST_RELAXED];
+        st->improved = u[ctl::ST_IMPROVED];
+        st->first_max = (uint32_t)u[ctl::ST_FIRST_MAX];
+        st->grid = b->grid;
+        st->block = 32 * (b->workers + 1);
+        st->status = c[ctl::STATUS];
+    }
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_batch_dist(mlmq_batch *b, int q, int **d_dist) {
+    if (!b || !d_dist || q < 0 || q >= b->max_q) return MLMQ_ERR_ARG;
+    *d_dist = b->d_dist + (size_t)q * b->max_n;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_batch_copy_dist(mlmq_batch *b, int q, int *h_dist) {
+    if (!b || !h_dist || q < 0 || q >= b->nq) return MLMQ_ERR_ARG;
+    int rc = cuda_fail(cudaMemcpyAsync(h_dist, b->d_dist + (size_t)q * b->max_n,
+                                       sizeof(int) * (size_t)b->n_of[q], cudaMemcpyDeviceToHost,
+                                       b->stream), "batch D2H");
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(b->stream), "batch D2H sync");
+    return rc;
+}
+
+extern "C" void mlmq_batch_destroy(mlmq_batch *b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    cudaFree(b->d_dist);
+    cudaFree(b->d_l2);
+    cudaFree(b->d_l3);
+    cudaFree(b->d_ctl);
+    cudaFree(b->d_params);
+    if (b->h_params) cudaFreeHost(b->h_params);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}

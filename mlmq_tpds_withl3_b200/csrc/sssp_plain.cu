@@ -6,7 +6,7 @@
 namespace mlmq {
 
 __global__ void __launch_bounds__(1024, 1) sssp_plain_kernel(PlainParams p) {
-    plain_body<ArcsInterleaved>(p);
+    plain_body<ArcsInterleaved>(p, blockIdx.x, gridDim.x);
 }
 
 // ---- host side ----------------------------------------------------------------

@@ -20,9 +20,8 @@
 namespace mlmq {
 
 __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirror &mir,
-                                             unsigned long long deadline) {
+                                             unsigned long long deadline, bool controller) {
     const int lane = threadIdx.x & 31;
-    const bool controller = blockIdx.x == 0;
     const int rings = p.nb + 1;  // buckets + urgent ring
     const unsigned cap8 = 1u << (p.l2_log - 3);
     unsigned ns = 64;
@@ -140,8 +139,10 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
     }
 }
 
+// `grank`/`gsize`: this CTA's rank in, and the size of, the group of CTAs
+// that serves the query (the whole grid for a single-source launch).
 template <class Arcs>
-__device__ __forceinline__ void plain_body(const PlainParams &p) {
+__device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank, unsigned gsize) {
     extern __shared__ uint2 smem[];
     __shared__ Mirror mir_storage;
     volatile Mirror &mir = mir_storage;
@@ -150,21 +151,21 @@ __device__ __forceinline__ void plain_body(const PlainParams &p) {
     const unsigned long long deadline = globaltimer() + p.timeout_ns;
 
     // ---- prologue: reset ------------------------------------------------------
-    const size_t gtid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t gstride = (size_t)gridDim.x * blockDim.x;
+    const size_t gtid = (size_t)grank * blockDim.x + threadIdx.x;
+    const size_t gstride = (size_t)gsize * blockDim.x;
     for (size_t i = gtid; i < (size_t)p.n; i += gstride) p.dist[i] = INT_MAX;
-    if (blockIdx.x == 0) {
+    if (grank == 0) {
         for (int i = threadIdx.x; i < ctl::WORDS; i += blockDim.x)
             if (i != ctl::BAR_COUNT && i != ctl::BAR_GEN) p.ctlw[i] = 0u;
     }
-    if (!grid_barrier(p.ctlw, gridDim.x, deadline)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!grid_barrier(p.ctlw, gsize, deadline)) return;
+    if (grank == 0 && threadIdx.x == 0) {
         p.dist[p.src] = 0;
         *l2_slot(p, 0, 0u) = rec_pack((unsigned)p.src, 0u, 0u);
         p.ctlw[ctl::RESERVE + 0] = 1u;
         p.ctlw[ctl::STATS + 2 * ctl::ST_PUSHED] = 1u;
     }
-    if (!grid_barrier(p.ctlw, gridDim.x, deadline)) return;
+    if (!grid_barrier(p.ctlw, gsize, deadline)) return;
 
     // ---- initial mirror ----------------------------------------------------------
     if (threadIdx.x < NB_MAX) {
@@ -181,7 +182,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p) {
     __syncthreads();
 
     if (warp == p.workers) {
-        manager_loop(p, mir, deadline);
+        manager_loop(p, mir, deadline, grank == 0);
         return;
     }
 

@@ -1,0 +1,490 @@
+// sssp_server.cu -- continuous-batching query server: one persistent launch
+// that keeps serving single-source queries on HBM-resident graphs while new
+// queries arrive.
+//
+// The grid is split into `slots` contiguous CTA groups (as in the batched
+// launch).  Each slot owns a distance buffer, queue rings and a control
+// block.  The host hands a query to a free slot by writing a command into
+// pinned host memory that the GPU reads directly (mapped); the slot's first
+// CTA polls it, publishes it to the rest of its group in device memory, and
+// the group runs the single-source algorithm (sssp_plain_body.cuh).  At the
+// end a group barrier makes sure every CTA of the slot has left the solve,
+// and the first CTA writes the completion (sequence number, status, counters)
+// into mapped host memory.  The host copies the distances out on another
+// stream while the server keeps running; the slot takes its next query once
+// that copy is done.  Queries on different graphs and of different sizes run
+// side by side; a query's result does not depend on what else runs.
+//
+// Every wait is bounded: by the server's lifetime deadline, by a host-set
+// shutdown flag, and inside a solve by the per-query time limit.
+#include "mlmq_b200.h"
+#include "solver_internal.h"
+#include "sssp_plain.h"
+#include "sssp_plain_body.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <vector>
+
+namespace mlmq {
+namespace {
+
+constexpr int SRV_CTL_STRIDE = 512;  // words per slot control block
+// Words of the slot control block used by the server around a solve (the
+// solve itself uses words below ctl::WORDS).
+constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs (2 words each), n, src
+constexpr int SRV_GO = 480;       // published command sequence (device)
+constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
+constexpr int SRV_BAR_COUNT = 488;
+constexpr int SRV_BAR_GEN = 489;
+
+__device__ __forceinline__ unsigned long long ld_acquire_sys64(const volatile unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Host-mapped command, one per slot, written by the host: every field first,
+// then `seq` (x86 stores become visible in program order).
+struct alignas(64) SlotCommand {
+    volatile unsigned long long seq;
+    const int *row;
+    const int2 *arcs;
+    int n;
+    int src;
+};
+// Host-mapped completion, one per slot, written by the device.
+struct alignas(64) SlotCompletion {
+    volatile unsigned long long seq;
+    volatile unsigned status;
+    volatile unsigned first_max;
+    volatile unsigned long long relaxed, pushed;
+};
+
+struct ServerParams {
+    PlainParams base;             // queue configuration shared by all slots
+    SlotCommand *cmd;             // mapped, [slots]
+    SlotCompletion *done;         // mapped, [slots]
+    volatile unsigned *shutdown;  // mapped
+    int *dist;                    // slots * max_n
+    unsigned long long *l2, *l3;
+    unsigned *ctl;                // slots * SRV_CTL_STRIDE
+    int slots, max_n;
+    unsigned long long lifetime_ns;
+};
+
+// Group barrier on words outside the solve's control words.
+__device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long deadline) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        unsigned gen = ld_acquire(c + SRV_BAR_GEN);
+        __threadfence();
+        if (atomicAdd(c + SRV_BAR_COUNT, 1u) == gsize - 1) {
+            st_relaxed(c + SRV_BAR_COUNT, 0u);
+            __threadfence();
+            st_release(c + SRV_BAR_GEN, gen + 1);
+        } else {
+            unsigned ns = 64;
+            while (ld_acquire(c + SRV_BAR_GEN) == gen) {
+                if (globaltimer() > deadline) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 2048) ns <<= 1;
+            }
+        }
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
+    const unsigned g = gridDim.x;
+    const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)sp.slots) / g);
+    const unsigned lo = (unsigned)(((unsigned long long)s * g + sp.slots - 1) / (unsigned)sp.slots);
+    const unsigned hi =
+        (unsigned)(((unsigned long long)(s + 1) * g + sp.slots - 1) / (unsigned)sp.slots);
+    const unsigned grank = blockIdx.x - lo, gsize = hi - lo;
+    unsigned *c = sp.ctl + (size_t)s * SRV_CTL_STRIDE;
+    const unsigned long long end = globaltimer() + sp.lifetime_ns;
+    __shared__ unsigned long long go_seq;
+    __shared__ int stop;
+    unsigned long long seen = 0;
+    for (;;) {
+        // ---- wait for the slot's next command ------------------------------
+        if (threadIdx.x == 0) {
+            stop = 0;
+            unsigned ns = 256;
+            for (;;) {
+                if (grank == 0) {
+                    if (*sp.shutdown) {
+                        st_release(c + SRV_STOP, 1u);
+                        stop = 1;
+                        break;
+                    }
+                    const unsigned long long q = ld_acquire_sys64(&sp.cmd[s].seq);
+                    if (q != seen) {
+                        go_seq = q;
+                        // Copy the command into device memory for the group.
+                        const unsigned long long row = (unsigned long long)sp.cmd[s].row;
+                        const unsigned long long arcs = (unsigned long long)sp.cmd[s].arcs;
+                        c[SRV_CMD + 0] = (unsigned)row;
+                        c[SRV_CMD + 1] = (unsigned)(row >> 32);
+                        c[SRV_CMD + 2] = (unsigned)arcs;
+                        c[SRV_CMD + 3] = (unsigned)(arcs >> 32);
+                        c[SRV_CMD + 4] = (unsigned)sp.cmd[s].n;
+                        c[SRV_CMD + 5] = (unsigned)sp.cmd[s].src;
+                        __threadfence();
+                        // publish the sequence number (low 32 bits) to the group
+                        st_release(c + SRV_GO, (unsigned)q);
+                        break;
+                    }
+                } else {
+                    if (ld_acquire(c + SRV_STOP)) {
+                        stop = 1;
+                        break;
+                    }
+                    const unsigned q = ld_acquire(c + SRV_GO);
+                    if (q != (unsigned)seen) {
+                        go_seq = seen + (unsigned)(q - (unsigned)seen);
+                        break;
+                    }
+                }
+                if (globaltimer() > end) {
+                    stop = 1;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 4096) ns <<= 1;
+            }
+        }
+        __syncthreads();
+        if (stop) return;
+        seen = go_seq;
+        // ---- one solve --------------------------------------------------------
+        PlainParams p = sp.base;
+        const volatile unsigned *cmd = c + SRV_CMD;
+        p.row = (const int *)(((unsigned long long)cmd[1] << 32) | cmd[0]);
+        p.arcs = (const int2 *)(((unsigned long long)cmd[3] << 32) | cmd[2]);
+        p.n = (int)cmd[4];
+        p.src = (int)cmd[5];
+        p.dist = sp.dist + (size_t)s * sp.max_n;
+        p.l2 = sp.l2 + ((size_t)s * (p.nb + 1) << p.l2_log);
+        p.l3 = sp.l3 + ((size_t)s << p.l3_log);
+        p.ctlw = c;
+        plain_body<ArcsInterleaved>(p, grank, gsize);
+        // A solve that stopped early leaves records in the rings: the group
+        // empties them before the slot is reused.
+        __shared__ unsigned solve_status;
+        if (threadIdx.x == 0) solve_status = ld_acquire(c + ctl::STATUS);
+        __syncthreads();
+        if (solve_status & (ST_TIMEOUT | ST_QUEUE_FULL)) {
+            if (!group_barrier(c, gsize, end)) return;
+            const size_t l2n = (size_t)(p.nb + 1) << p.l2_log, l3n = (size_t)1 << p.l3_log;
+            for (size_t i = (size_t)grank * blockDim.x + threadIdx.x; i < l2n + l3n;
+                 i += (size_t)gsize * blockDim.x) {
+                if (i < l2n) p.l2[i] = SENT;
+                else p.l3[i - l2n] = SENT;
+            }
+        }
+        // Every CTA of the slot has left the solve before it is reported.
+        const bool ok = group_barrier(c, gsize, end);
+        if (grank == 0 && threadIdx.x == 0) {
+            const unsigned long long *u = reinterpret_cast<const unsigned long long *>(c + ctl::STATS);
+            unsigned st = ld_acquire(c + ctl::STATUS);
+            if (!ok) st |= ST_TIMEOUT;
+            sp.done[s].status = st;
+            sp.done[s].first_max = (unsigned)u[ctl::ST_FIRST_MAX];
+            sp.done[s].relaxed = u[ctl::ST_RELAXED];
+            sp.done[s].pushed = u[ctl::ST_PUSHED];
+            __threadfence_system();
+            sp.done[s].seq = seen;
+            __threadfence_system();
+        }
+        if (!ok) return;
+    }
+}
+
+}  // namespace
+}  // namespace mlmq
+
+using namespace mlmq;
+
+struct mlmq_server {
+    int device = 0;
+    mlmq_config cfg{};
+    int slots = 0, max_n = 0, grid = 0, workers = 0, l2_log = 0, l3_log = 0;
+    int *d_dist = nullptr;
+    unsigned long long *d_l2 = nullptr, *d_l3 = nullptr;
+    unsigned *d_ctl = nullptr;
+    SlotCommand *h_cmd = nullptr;
+    SlotCompletion *h_done = nullptr;
+    unsigned *h_shutdown = nullptr;
+    cudaStream_t kstream = nullptr, cstream = nullptr;
+    cudaEvent_t kdone = nullptr;
+    bool running = false;
+    std::mutex mu;
+    struct Slot {
+        unsigned long long seq = 0;     // last command issued
+        bool busy = false;              // solving or copying out
+        bool copying = false;
+        unsigned long long ticket = 0;
+        int *h_out = nullptr;
+        int n = 0;
+        cudaEvent_t copied = nullptr;
+        unsigned status = 0;
+        unsigned long long relaxed = 0;
+    };
+    std::vector<Slot> st;
+    unsigned long long next_ticket = 1;
+    std::deque<std::pair<unsigned long long, int>> finished;  // (ticket, status)
+};
+
+extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config *cfg_in,
+                                  int lifetime_ms, mlmq_server **out) {
+    if (!out || slots < 1 || max_vertices < 1 || lifetime_ms < 1) return MLMQ_ERR_ARG;
+    mlmq_config cfg;
+    int rc = MLMQ_OK;
+    if (cfg_in) cfg = *cfg_in;
+    else {
+        if ((rc = mlmq_config_default(&cfg))) return rc;
+        cfg.warps_per_block = 8;
+    }
+    if ((rc = validate_config(cfg))) return rc;
+    int sms = 0;
+    if ((rc = device_sm_count(&sms))) return rc;
+    auto *sv = new (std::nothrow) mlmq_server;
+    if (!sv) return MLMQ_ERR_NOMEM;
+    sv->cfg = cfg;
+    sv->workers = cfg.warps_per_block;
+    sv->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : MLMQ_MIN_RING_LOG2;
+    sv->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : MLMQ_MIN_RING_LOG2 + 2;
+    sv->max_n = max_vertices;
+    rc = cuda_fail(cudaGetDevice(&sv->device), "cudaGetDevice");
+    // Admission by free device memory: as many slots as fit after a reserve.
+    const size_t per_slot = sizeof(int) * (size_t)max_vertices +
+                            8 * (((size_t)(cfg.bucket_num + 1) << sv->l2_log) + ((size_t)1 << sv->l3_log)) +
+                            4 * SRV_CTL_STRIDE;
+    size_t free_b = 0, total_b = 0;
+    if (!rc) rc = cuda_fail(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    if (!rc) {
+        const size_t reserve = (size_t)2 << 30;
+        const size_t fit = free_b > reserve ? (free_b - reserve) / per_slot : 0;
+        sv->slots = (int)std::min<size_t>((size_t)slots, fit);
+        if (sv->slots < 1) rc = MLMQ_ERR_NOMEM;
+    }
+    int bps = 0;
+    const int threads = 32 * (sv->workers + 1);
+    const size_t smem = plain_smem_bytes(sv->workers);
+    if (!rc) rc = cuda_fail(cudaFuncSetAttribute(sssp_server_kernel,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem), "server smem");
+    if (!rc) rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_server_kernel,
+                                                                          threads, smem),
+                            "server occupancy");
+    if (!rc) {
+        sv->grid = cfg.work_blocks > 0 ? std::min(cfg.work_blocks, bps * sms) : bps * sms;
+        sv->slots = std::min(sv->slots, sv->grid);
+    }
+    const size_t ns = (size_t)sv->slots;
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_dist, sizeof(int) * ns * (size_t)max_vertices), "server dist");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l2, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log)), "server L2");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3, 8 * (ns << sv->l3_log)), "server L3");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_ctl, 4 * ns * SRV_CTL_STRIDE), "server ctl");
+    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_cmd, sizeof(SlotCommand) * ns, cudaHostAllocMapped), "cmd");
+    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_done, sizeof(SlotCompletion) * ns, cudaHostAllocMapped), "done");
+    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_shutdown, 64, cudaHostAllocMapped), "shutdown");
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking), "kstream");
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "cstream");
+    if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&sv->kdone, cudaEventDisableTiming), "kdone");
+    if (!rc) {
+        std::memset((void *)sv->h_cmd, 0, sizeof(SlotCommand) * ns);
+        std::memset((void *)sv->h_done, 0, sizeof(SlotCompletion) * ns);
+        *sv->h_shutdown = 0;
+        sv->st.resize(ns);
+        for (auto &sl : sv->st)
+            if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming), "copy event");
+    }
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_l2, 0xff, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log), sv->kstream), "reset L2");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_l3, 0xff, 8 * (ns << sv->l3_log), sv->kstream), "reset L3");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_ctl, 0, 4 * ns * SRV_CTL_STRIDE, sv->kstream), "reset ctl");
+    if (!rc) {
+        ServerParams sp{};
+        PlainParams &b = sp.base;
+        b.nb = cfg.bucket_num;
+        b.bm = cfg.bucket_max;
+        b.batch = cfg.l2_batch;
+        b.min_read = cfg.min_read;
+        b.large = cfg.large_degree;
+        b.l1_spill = cfg.l1_spill;
+        b.l1_vector = cfg.queue_type == MLMQ_L1V_L2DQ;
+        b.delta = (unsigned)cfg.delta;
+        b.l2_log = sv->l2_log;
+        b.l3_log = sv->l3_log;
+        b.workers = sv->workers;
+        b.timeout_ns = (unsigned long long)cfg.timeout_ms * 1000000ull;
+        void *p_cmd = nullptr, *p_done = nullptr, *p_stop = nullptr;
+        rc = cuda_fail(cudaHostGetDevicePointer(&p_cmd, sv->h_cmd, 0), "map cmd");
+        if (!rc) rc = cuda_fail(cudaHostGetDevicePointer(&p_done, sv->h_done, 0), "map done");
+        if (!rc) rc = cuda_fail(cudaHostGetDevicePointer(&p_stop, sv->h_shutdown, 0), "map stop");
+        sp.cmd = (SlotCommand *)p_cmd;
+        sp.done = (SlotCompletion *)p_done;
+        sp.shutdown = (volatile unsigned *)p_stop;
+        sp.dist = sv->d_dist;
+        sp.l2 = sv->d_l2;
+        sp.l3 = sv->d_l3;
+        sp.ctl = sv->d_ctl;
+        sp.slots = sv->slots;
+        sp.max_n = max_vertices;
+        sp.lifetime_ns = (unsigned long long)lifetime_ms * 1000000ull;
+        if (!rc) {
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3((unsigned)sv->grid);
+            lc.blockDim = dim3((unsigned)threads);
+            lc.dynamicSmemBytes = smem;
+            lc.stream = sv->kstream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            lc.attrs = attr;
+            lc.numAttrs = 1;
+            rc = cuda_fail(cudaLaunchKernelEx(&lc, sssp_server_kernel, sp), "server launch");
+        }
+        if (!rc) rc = cuda_fail(cudaEventRecord(sv->kdone, sv->kstream), "server event");
+        sv->running = !rc;
+    }
+    if (rc) {
+        mlmq_server_destroy(sv);
+        return rc;
+    }
+    *out = sv;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block) {
+    if (!sv) return MLMQ_ERR_ARG;
+    if (slots) *slots = sv->slots;
+    if (grid) *grid = sv->grid;
+    if (block) *block = 32 * (sv->workers + 1);
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
+                                  uint64_t *ticket) {
+    if (!sv || !g || !h_out || !ticket || src < 0 || src >= g->n || g->n > sv->max_n)
+        return MLMQ_ERR_ARG;
+    if (g->device != sv->device) return MLMQ_ERR_ARG;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!sv->running) return MLMQ_ERR_STATE;
+    int free_slot = -1;
+    for (int s = 0; s < sv->slots; s++)
+        if (!sv->st[s].busy) {
+            free_slot = s;
+            break;
+        }
+    if (free_slot < 0) return MLMQ_ERR_BUSY;
+    auto &sl = sv->st[free_slot];
+    SlotCommand &cmd = sv->h_cmd[free_slot];
+    cmd.row = g->d_row;
+    cmd.arcs = g->d_arcs;
+    cmd.n = g->n;
+    cmd.src = src;
+    std::atomic_thread_fence(std::memory_order_release);
+    sl.seq++;
+    sl.busy = true;
+    sl.copying = false;
+    sl.ticket = sv->next_ticket++;
+    sl.h_out = h_out;
+    sl.n = g->n;
+    cmd.seq = sl.seq;  // published last
+    *ticket = sl.ticket;
+    return MLMQ_OK;
+}
+
+// Moves finished solves to the copy stream and retires finished copies.
+extern "C" int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max,
+                                int *count) {
+    if (!sv || !count || (max > 0 && (!tickets || !statuses))) return MLMQ_ERR_ARG;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    int rc = MLMQ_OK;
+    for (int s = 0; s < sv->slots; s++) {
+        auto &sl = sv->st[s];
+        if (!sl.busy) continue;
+        if (!sl.copying) {
+            if (sv->h_done[s].seq != sl.seq) continue;
+            std::atomic_thread_fence(std::memory_order_acquire);
+            sl.status = sv->h_done[s].status;
+            sl.relaxed = sv->h_done[s].relaxed;
+            rc = cuda_fail(cudaMemcpyAsync(sl.h_out, sv->d_dist + (size_t)s * sv->max_n,
+                                           sizeof(int) * (size_t)sl.n, cudaMemcpyDeviceToHost,
+                                           sv->cstream), "server D2H");
+            if (!rc) rc = cuda_fail(cudaEventRecord(sl.copied, sv->cstream), "copy event");
+            if (rc) return rc;
+            sl.copying = true;
+        } else if (cudaEventQuery(sl.copied) == cudaSuccess) {
+            sl.busy = false;
+            sl.copying = false;
+            sv->finished.emplace_back(sl.ticket, status_to_error(sl.status));
+        }
+    }
+    int k = 0;
+    while (k < max && !sv->finished.empty()) {
+        tickets[k] = sv->finished.front().first;
+        statuses[k] = sv->finished.front().second;
+        sv->finished.pop_front();
+        k++;
+    }
+    *count = k;
+    // The server kernel ending early (lifetime or an error) is reported too.
+    if (sv->running && cudaEventQuery(sv->kdone) == cudaSuccess) sv->running = false;
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_server_busy_slots(mlmq_server *sv, int *busy) {
+    if (!sv || !busy) return MLMQ_ERR_ARG;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    int b = 0;
+    for (auto &sl : sv->st) b += sl.busy;
+    *busy = b;
+    return sv->running ? MLMQ_OK : MLMQ_ERR_STATE;
+}
+
+extern "C" int mlmq_server_stop(mlmq_server *sv) {
+    if (!sv) return MLMQ_ERR_ARG;
+    if (sv->h_shutdown) {
+        *(volatile unsigned *)sv->h_shutdown = 1;
+        std::atomic_thread_fence(std::memory_order_seq_cst);
+    }
+    int rc = MLMQ_OK;
+    if (sv->kstream) rc = cuda_fail(cudaStreamSynchronize(sv->kstream), "server stop");
+    if (sv->cstream) cudaStreamSynchronize(sv->cstream);
+    sv->running = false;
+    return rc;
+}
+
+extern "C" void mlmq_server_destroy(mlmq_server *sv) {
+    if (!sv) return;
+    mlmq_server_stop(sv);
+    for (auto &sl : sv->st)
+        if (sl.copied) cudaEventDestroy(sl.copied);
+    cudaFree(sv->d_dist);
+    cudaFree(sv->d_l2);
+    cudaFree(sv->d_l3);
+    cudaFree(sv->d_ctl);
+    if (sv->h_cmd) cudaFreeHost(sv->h_cmd);
+    if (sv->h_done) cudaFreeHost(sv->h_done);
+    if (sv->h_shutdown) cudaFreeHost(sv->h_shutdown);
+    if (sv->kdone) cudaEventDestroy(sv->kdone);
+    if (sv->kstream) cudaStreamDestroy(sv->kstream);
+    if (sv->cstream) cudaStreamDestroy(sv->cstream);
+    delete sv;
+}

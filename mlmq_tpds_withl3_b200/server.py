@@ -1,0 +1,143 @@
+"""Continuous-batching query server and a Poisson load generator.
+
+``Server`` wraps mlmq_server_*: one persistent launch on the GPU serves
+single-source queries on HBM-resident graphs while new ones arrive; each
+query takes a free slot (a group of CTAs with its own distance array and
+queues), runs alongside the other slots' queries, and its distances are
+copied into a pinned host buffer when it finishes.
+
+``serve_poisson`` drives a server with Poisson arrivals (each query picks a
+graph uniformly and a source uniformly) and measures per-query latency
+(finish - arrival, host clock) and throughput.
+"""
+import ctypes
+import time
+from collections import deque
+
+import numpy as np
+
+from . import _lib
+from ._lib import MLMQ_ERR_BUSY, check, lib
+
+
+class Server:
+    def __init__(self, slots, max_vertices, cfg=None, lifetime_s=600.0):
+        if cfg is None or isinstance(cfg, dict):
+            cfg = _lib.default_config(**{"warps_per_block": 8, **(cfg or {})})
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        check(lib.mlmq_server_create(slots, max_vertices, ctypes.byref(cfg),
+                                     int(lifetime_s * 1000), ctypes.byref(h)), "mlmq_server_create")
+        self._h = h
+        s, g, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib.mlmq_server_info(h, ctypes.byref(s), ctypes.byref(g), ctypes.byref(b)))
+        self.slots, self.grid, self.block = s.value, g.value, b.value
+        self.max_vertices = max_vertices
+        self._tk = (ctypes.c_uint64 * 256)()
+        self._st = (ctypes.c_int * 256)()
+
+    def submit(self, dgraph, src, out):
+        """Returns a ticket, or None when every slot is busy.  `out` must be a
+        host int32 buffer of dgraph.n entries (pinned for asynchronous copy)
+        that stays alive until the ticket completes."""
+        t = ctypes.c_uint64()
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        rc = lib.mlmq_server_submit(self._h, dgraph.handle, int(src), ptr, ctypes.byref(t))
+        if rc == MLMQ_ERR_BUSY:
+            return None
+        check(rc, "mlmq_server_submit")
+        return t.value
+
+    def poll(self):
+        """[(ticket, status)] of queries whose distances are now on the host."""
+        n = ctypes.c_int()
+        check(lib.mlmq_server_poll(self._h, self._tk, self._st, 256, ctypes.byref(n)),
+              "mlmq_server_poll")
+        return [(self._tk[i], self._st[i]) for i in range(n.value)]
+
+    def busy(self):
+        b = ctypes.c_int()
+        rc = lib.mlmq_server_busy_slots(self._h, ctypes.byref(b))
+        return b.value, rc == 0
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib.mlmq_server_destroy(self._h)
+        self._h = None
+
+    __del__ = close
+
+
+class PinnedPool:
+    """Pinned host buffers of `size` int32, one per in-flight query."""
+
+    def __init__(self, count, size):
+        import torch
+        self.free = [torch.empty(size, dtype=torch.int32, pin_memory=True)
+                     for _ in range(count)]
+
+    def get(self):
+        return self.free.pop() if self.free else None
+
+    def put(self, buf):
+        self.free.append(buf)
+
+
+def poisson_schedule(rate, count, graphs_n, seed=1):
+    """(arrival_s, graph_index, source) for `count` queries at `rate`/s."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    gi = rng.integers(0, len(graphs_n), size=count)
+    src = [int(rng.integers(0, graphs_n[i])) for i in gi]
+    return list(zip(t.tolist(), gi.tolist(), src))
+
+
+def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0):
+    """Runs the schedule against the server.  Returns a list of dicts
+    (arrival, start, finish, latency_s, graph, src, status[, dist]) in
+    schedule order; `keep(i)` selects the queries whose distances are kept."""
+    pool = pool or PinnedPool(server.slots, max(g.n for g in dgraphs))
+    pending = deque(range(len(schedule)))
+    inflight = {}
+    out = [None] * len(schedule)
+    t0 = time.perf_counter()
+    while pending or inflight:
+        now = time.perf_counter() - t0
+        if now > timeout_s:
+            raise TimeoutError("serving did not finish in time")
+        # admit every arrived query while a slot and a buffer are free
+        while pending and schedule[pending[0]][0] <= now:
+            i = pending[0]
+            buf = pool.get()
+            if buf is None:
+                break
+            _, gi, src = schedule[i]
+            tk = server.submit(dgraphs[gi], src, buf)
+            if tk is None:
+                pool.put(buf)
+                break
+            pending.popleft()
+            inflight[tk] = (i, buf, now)
+        for tk, status in server.poll():
+            i, buf, start = inflight.pop(tk)
+            arr, gi, src = schedule[i]
+            fin = time.perf_counter() - t0
+            rec = {"arrival": arr, "start": start, "finish": fin, "latency_s": fin - arr,
+                   "graph": gi, "src": src, "status": status}
+            if keep is not None and keep(i):
+                rec["dist"] = buf[:dgraphs[gi].n].numpy().copy()
+            out[i] = rec
+            pool.put(buf)
+        if not inflight and pending:
+            wait = schedule[pending[0]][0] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(min(wait, 0.001))
+    return out
+
+
+def summarize(records):
+    lat = np.array([r["latency_s"] for r in records]) * 1e3
+    span = max(r["finish"] for r in records) - min(r["arrival"] for r in records)
+    return {"queries": len(records), "qps": len(records) / span,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "errors": sum(1 for r in records if r["status"])}

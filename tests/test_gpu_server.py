@@ -1,0 +1,61 @@
+"""Continuous-batching server: queries on graphs of different sizes arrive
+while others run; every result equals the oracle and the same query solved
+alone."""
+import numpy as np
+import pytest
+
+import oracle_lib
+from mlmq_tpds_withl3_b200 import DeviceGraph, HostGraph, Solver
+from mlmq_tpds_withl3_b200.server import Server, poisson_schedule, serve_poisson, summarize
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs():
+    return [HostGraph.grid(128, 128, seed=41), HostGraph.grid(300, 260, seed=42),
+            HostGraph.knn(30000, seed=43), HostGraph.rmat(13, seed=44)]
+
+
+def test_served_results_equal_oracle_and_alone():
+    hgs = _graphs()
+    dgs = [DeviceGraph.upload(g) for g in hgs]
+    sv = Server(slots=12, max_vertices=max(g.n for g in hgs), lifetime_s=120)
+    sched = poisson_schedule(rate=3000.0, count=80, graphs_n=[g.n for g in hgs], seed=7)
+    recs = serve_poisson(sv, dgs, sched, keep=lambda i: True, timeout_s=60)
+    sv.close()
+    assert all(r["status"] == 0 for r in recs)
+    # queries overlapped on the device: some started before others finished
+    overlap = sum(1 for a, b in zip(recs, recs[1:]) if b["start"] < a["finish"])
+    assert overlap > 0
+    alone = [Solver(dg) for dg in dgs]
+    for i, r in enumerate(recs):
+        gi, src = r["graph"], r["src"]
+        solo = alone[gi].solve(src).dist()
+        assert np.array_equal(r["dist"], solo), (i, gi, src)
+        if i % 5 == 0:
+            ref, _ = oracle_lib.sssp_i32(hgs[gi], src)
+            assert np.array_equal(r["dist"], ref), (i, gi, src)
+    s = summarize(recs)
+    assert s["errors"] == 0 and s["queries"] == 80
+
+
+def test_server_busy_and_stop():
+    g = HostGraph.grid(64, 64, seed=45)
+    dg = DeviceGraph.upload(g)
+    import torch
+    sv = Server(slots=2, max_vertices=g.n, lifetime_s=60)
+    bufs = [torch.empty(g.n, dtype=torch.int32, pin_memory=True) for _ in range(3)]
+    t1 = sv.submit(dg, 0, bufs[0])
+    t2 = sv.submit(dg, 1, bufs[1])
+    assert t1 is not None and t2 is not None
+    assert sv.submit(dg, 2, bufs[2]) is None  # both slots busy
+    done = {}
+    import time
+    t0 = time.time()
+    while len(done) < 2 and time.time() - t0 < 30:
+        for tk, st in sv.poll():
+            done[tk] = st
+    assert done == {t1: 0, t2: 0}
+    ref0, _ = oracle_lib.sssp_i32(g, 0)
+    assert np.array_equal(bufs[0].numpy(), ref0)
+    sv.close()
