@@ -81,6 +81,10 @@ typedef struct mlmq_config {
     int l3_cap_log2;     /* log2 slots of the L3 ring; 0 = sized from graph;
                             else MLMQ_MIN_RING_LOG2..30 */
     int timeout_ms;      /* device wait limit per solve (default 20000) */
+    int l1_keep;         /* on a spill, records kept at the L1 front (0 = spill
+                            all, the reference's rule; at most l1_spill) */
+    int relax_precheck;  /* 1: read dist[dst] before atomicMin (default);
+                            0: atomicMin directly (one less dependent load) */
 } mlmq_config;
 
 /* Fills *cfg with the reference's defaults (common.h:24-34, sssp.cuh:20,
@@ -145,6 +149,19 @@ int mlmq_hgraph_from_csr(int n, int64_t m, const int *row, const int *col,
 /* Galois/LonestarGPU .gr v1 (SSSP/csr_graph.cu:185-300, 302-418). */
 int mlmq_hgraph_read_gr(const char *path, mlmq_host_graph **out);
 int mlmq_hgraph_write_gr(const mlmq_host_graph *g, const char *path);
+/* BFS locality reordering (graph_transform/reorder_gr.cu:96-190): new ids in
+ * the discovery order of a queue BFS from root (arcs scanned in CSR order),
+ * unreached vertices after them in ascending id; perm[new] = old,
+ * invperm[old] = new (n entries each, may be NULL). */
+int mlmq_hgraph_reorder_bfs(const mlmq_host_graph *g, int root, mlmq_host_graph **out,
+                            int *perm, int *invperm);
+/* Chain-shortcut augmentation G+ (SSSP/l3/l3_chain_shortcuts.h:23-109):
+ * adds one arc per maximal walk through degree-2 chain vertices, keeps every
+ * original arc, so distances are unchanged.  cut = n places no partition
+ * restriction; stats (may be NULL): chain vertices, shortcuts, longest walk,
+ * walks dropped for INT_MAX overflow, arcs represented. */
+int mlmq_hgraph_chain_shortcuts(const mlmq_host_graph *g, int cut, int source,
+                                mlmq_host_graph **out, int64_t *stats);
 /* Borrowed views; valid until mlmq_hgraph_free.  perm may be NULL. */
 int mlmq_hgraph_view(const mlmq_host_graph *g, int *n, int64_t *m, const int **row,
                      const int **col, const int **w, const int **perm);
@@ -278,7 +295,7 @@ void mlmq_server_destroy(mlmq_server *sv);
  *    two streams) race and corrupt each other's results.  Serialise them. */
 #define MLMQ_NOALLOC_MAX_VERTICES (1 << 20)
 #define MLMQ_NOALLOC_MAX_ARCS (1 << 20)
-#define MLMQ_NOALLOC_WORKSPACE_BYTES 26215744
+#define MLMQ_NOALLOC_WORKSPACE_BYTES 26346816
 int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int *d_col, const int *d_w,
                             int src, int *d_dist, const mlmq_config *cfg, void *stream);
 

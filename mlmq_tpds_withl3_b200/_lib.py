@@ -60,7 +60,7 @@ class Config(ctypes.Structure):
     _fields_ = [(n, c_int) for n in (
         "queue_type", "delta", "work_blocks", "warps_per_block", "l2_batch",
         "bucket_num", "bucket_max", "min_read", "large_degree", "l1_spill",
-        "l2_cap_log2", "l3_cap_log2", "timeout_ms")]
+        "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -104,6 +104,8 @@ _sig("mlmq_hgraph_write_gr", c_int, c_vp, c_char_p)
 _sig("mlmq_hgraph_view", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_i64),
      ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), ctypes.POINTER(c_vp))
 _sig("mlmq_hgraph_free", None, c_vp)
+_sig("mlmq_hgraph_reorder_bfs", c_int, c_vp, c_int, ctypes.POINTER(c_vp), c_vp, c_vp)
+_sig("mlmq_hgraph_chain_shortcuts", c_int, c_vp, c_int, c_int, ctypes.POINTER(c_vp), c_vp)
 # device graphs / solver
 _sig("mlmq_graph_upload", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp))
 _sig("mlmq_graph_wrap_device", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp))

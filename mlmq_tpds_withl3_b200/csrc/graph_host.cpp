@@ -512,4 +512,181 @@ int mlmq_hgraph_view(const mlmq_host_graph *g, int *n, int64_t *m, const int **r
 
 void mlmq_hgraph_free(mlmq_host_graph *g) { delete g; }
 
+// BFS locality order (reference graph_transform/reorder_gr.cu:96-130,
+// 161-190): vertices numbered in the discovery order of a queue BFS from
+// `root` that scans arcs in CSR order; vertices never reached follow in
+// ascending original id.  Rows keep their arcs in the original order with the
+// destinations renumbered.  perm[new] = old and invperm[old] = new (each n
+// entries, optional).
+int mlmq_hgraph_reorder_bfs(const mlmq_host_graph *g, int root, mlmq_host_graph **out, int *perm,
+                            int *invperm) {
+    if (!g || !out || root < 0 || root >= g->n) return MLMQ_ERR_ARG;
+    auto *r = new (std::nothrow) mlmq_host_graph;
+    if (!r) return MLMQ_ERR_NOMEM;
+    try {
+        const int n = g->n;
+        std::vector<int> p((size_t)n), inv((size_t)n, -1), q((size_t)n);
+        int head = 0, tail = 0, next = 0;
+        q[tail++] = root;
+        inv[root] = next;
+        p[next++] = root;
+        while (head < tail) {
+            const int u = q[head++];
+            for (int e = g->row[u]; e < g->row[u + 1]; e++) {
+                const int v = g->col[e];
+                if (inv[v] == -1) {
+                    inv[v] = next;
+                    p[next++] = v;
+                    q[tail++] = v;
+                }
+            }
+        }
+        for (int v = 0; v < n; v++)
+            if (inv[v] == -1) {
+                inv[v] = next;
+                p[next++] = v;
+            }
+        r->n = n;
+        r->m = g->m;
+        r->row.assign((size_t)n + 1, 0);
+        for (int i = 0; i < n; i++) r->row[i + 1] = r->row[i] + (g->row[p[i] + 1] - g->row[p[i]]);
+        r->col.resize((size_t)g->m);
+        r->w.resize((size_t)g->m);
+        parallel_for(n, [&](int64_t b, int64_t e, int) {
+            for (int64_t i = b; i < e; i++) {
+                int pos = r->row[i];
+                for (int a = g->row[p[i]]; a < g->row[p[i] + 1]; a++, pos++) {
+                    r->col[pos] = inv[g->col[a]];
+                    r->w[pos] = g->w[a];
+                }
+            }
+        });
+        if (perm) std::copy(p.begin(), p.end(), perm);
+        if (invperm) std::copy(inv.begin(), inv.end(), invperm);
+    } catch (...) {
+        delete r;
+        return MLMQ_ERR_NOMEM;
+    }
+    *out = r;
+    return MLMQ_OK;
+}
+
+// Chain-shortcut augmentation G+ (reference SSSP/l3/l3_chain_shortcuts.h:
+// 23-109, strict variant).  A vertex is a chain vertex when it is not the
+// source, has exactly two out-arcs to two distinct other vertices on its own
+// side of `cut`, and exactly two in-arcs, which come from those same two
+// vertices.  From every other vertex, each out-arc is followed through chain
+// vertices to the first non-chain vertex; when that walk passes at least one
+// chain vertex, does not return to its start and its weight sum stays below
+// INT_MAX, one shortcut arc (start -> end, summed weight) is added before the
+// vertex's original arcs.  Every original arc is kept, so shortest-path
+// distances are unchanged.  stats (optional, 5 entries): chain vertices,
+// shortcuts, longest walk in arcs, walks dropped for overflow, arcs replaced.
+int mlmq_hgraph_chain_shortcuts(const mlmq_host_graph *g, int cut, int source,
+                                mlmq_host_graph **out, int64_t *stats) {
+    if (!g || !out) return MLMQ_ERR_ARG;
+    const int n = g->n;
+    const int64_t m = g->m;
+    if (source < 0 || source >= n || cut < 0 || cut > n) return MLMQ_ERR_ARG;
+    auto *r = new (std::nothrow) mlmq_host_graph;
+    if (!r) return MLMQ_ERR_NOMEM;
+    int rc = MLMQ_OK;
+    try {
+        const int *row = g->row.data(), *dst = g->col.data(), *wt = g->w.data();
+        std::vector<unsigned char> chain((size_t)n, 0);
+        std::vector<int> incoming((size_t)n, 0), rev0((size_t)n, -1), rev1((size_t)n, -1);
+        for (int u = 0; u < n; u++) {
+            if (u == source || row[u + 1] - row[u] != 2) continue;
+            const int a = dst[row[u]], b = dst[row[u] + 1];
+            chain[u] = a != u && b != u && a != b && (a < cut) == (u < cut) && (b < cut) == (u < cut);
+        }
+        for (int u = 0; u < n; u++)
+            for (int e = row[u]; e < row[u + 1]; e++) {
+                const int v = dst[e];
+                if (!chain[v]) continue;
+                ++incoming[v];
+                if (u == dst[row[v]]) rev0[v] = e;
+                if (u == dst[row[v] + 1]) rev1[v] = e;
+            }
+        int64_t nchain = 0, nshort = 0, longest = 0, overflow = 0, replaced = 0;
+        for (int u = 0; u < n; u++) {
+            chain[u] = chain[u] && incoming[u] == 2 && rev0[u] >= 0 && rev1[u] >= 0;
+            nchain += chain[u];
+        }
+        r->n = n;
+        r->row.assign((size_t)n + 1, 0);
+        r->col.reserve((size_t)m);
+        r->w.reserve((size_t)m);
+        for (int u = 0; u < n && !rc; u++) {
+            if (!chain[u])
+                for (int first = row[u]; first < row[u + 1]; first++) {
+                    int prev = u, cur = dst[first];
+                    int64_t hops = 1, cost = wt[first];
+                    bool over = false;
+                    while (chain[cur]) {
+                        int e = row[cur];
+                        if (dst[e] == prev) ++e;
+                        else if (dst[e + 1] != prev) {
+                            rc = MLMQ_ERR_ARG;  // cannot happen for a valid chain vertex
+                            break;
+                        }
+                        cost += wt[e];
+                        ++hops;
+                        prev = cur;
+                        cur = dst[e];
+                        if (cost >= INT_MAX) {
+                            over = true;
+                            break;
+                        }
+                        if (hops > n) {
+                            rc = MLMQ_ERR_ARG;
+                            break;
+                        }
+                    }
+                    if (rc) break;
+                    if (over) {
+                        ++overflow;
+                        continue;
+                    }
+                    if (hops <= 1 || cur == u) continue;
+                    if ((cur < cut) != (u < cut)) {
+                        rc = MLMQ_ERR_ARG;
+                        break;
+                    }
+                    if ((int64_t)r->col.size() >= INT_MAX) {
+                        rc = MLMQ_ERR_RANGE;
+                        break;
+                    }
+                    r->col.push_back(cur);
+                    r->w.push_back((int)cost);
+                    ++nshort;
+                    replaced += hops;
+                    longest = std::max(longest, hops);
+                }
+            for (int e = row[u]; e < row[u + 1]; e++) {
+                r->col.push_back(dst[e]);
+                r->w.push_back(wt[e]);
+            }
+            if ((int64_t)r->col.size() >= INT_MAX) rc = MLMQ_ERR_RANGE;
+            r->row[u + 1] = (int)r->col.size();
+        }
+        r->m = (int64_t)r->col.size();
+        if (stats) {
+            stats[0] = nchain;
+            stats[1] = nshort;
+            stats[2] = longest;
+            stats[3] = overflow;
+            stats[4] = replaced;
+        }
+    } catch (...) {
+        rc = MLMQ_ERR_NOMEM;
+    }
+    if (rc) {
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return MLMQ_OK;
+}
+
 }  // extern "C"

@@ -39,7 +39,12 @@
 //  * L3.  Records beyond the bucket window (the reference clamps them into
 //    the last bucket) and records for a bucket whose ring is filling go to
 //    one HBM ring shared by every CTA.  Warps read it when every L2 bucket is
-//    empty and move `first` up to the batch they took.
+//    empty and move `first` up to the batch they took.  L3 keeps at most one
+//    record per vertex: a per-vertex bit marks "has an L3 record", a push
+//    finding the bit set is dropped, and an L3 record is relaxed with the
+//    vertex's distance at read time (never filtered as stale), so the
+//    dropped improvement is applied.  L3 therefore never holds more than n
+//    records plus the pushes in flight, which bounds every queue level.
 //  * Every wait is bounded by a deadline and ends with a status bit, never a
 //    trap or an endless spin.
 #pragma once
@@ -58,8 +63,11 @@ struct PlainParams {
     int src;
     unsigned long long *l2;  // (nb + 1) rings of 2^l2_log slots; ring nb is the urgent ring
     unsigned long long *l3;  // 2^l3_log slots
+    unsigned *l3bits;        // one bit per vertex: the vertex has a record in L3
     unsigned *ctlw;
     int nb, bm, batch, min_read, large, l1_spill, l1_vector;
+    int l1_keep;   // records kept at the L1 front when it spills (0: spill all)
+    int precheck;  // read dist[dst] before the atomicMin
     unsigned delta;
     int l2_log, l3_log;
     int workers;  // worker warps per CTA (one more warp per CTA is the manager)
@@ -120,8 +128,7 @@ static __device__ __noinline__ void install_slow(const PlainParams &p, unsigned 
 // floor(d/delta) mod nb inside the window, L3 beyond it or under pressure.
 __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool valid, unsigned v,
                                        unsigned d) {
-    const unsigned act = __ballot_sync(FULL, valid);
-    if (!act) return;
+    if (!__ballot_sync(FULL, valid)) return;
     const int lane = threadIdx.x & 31;
     const unsigned f = ld_relaxed(p.ctlw + ctl::FIRST);
     const unsigned pres = ld_relaxed(p.ctlw + ctl::PRESSURE);
@@ -137,6 +144,20 @@ __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool vali
             tgt = ((pres >> b) & 1u) ? NB_MAX : b;
         }
     }
+    if (tgt == NB_MAX) {
+        // One L3 record per vertex.  The fence orders the atomicMin that made
+        // this record before the bit test: a reader that clears the bit after
+        // this atomicOr and then reads dist[v] sees the improvement, so a
+        // push dropped here loses nothing.
+        __threadfence();
+        const unsigned bit = 1u << (v & 31u);
+        if (atomicOr(p.l3bits + (v >> 5), bit) & bit) {
+            valid = false;
+            tgt = -1;
+        }
+    }
+    const unsigned act = __ballot_sync(FULL, valid);
+    if (!act) return;
     const unsigned grp = __match_any_sync(FULL, tgt);
     const int leader = __ffs(grp) - 1;
     const unsigned rank = __popc(grp & lanemask_lt());
@@ -195,8 +216,11 @@ __device__ __forceinline__ void l1_write(const PlainParams &p, WarpQ &q, uint2 *
     q.l1_tail = (q.l1_tail + (int)__popc(rm)) & (L1_CAP - 1);
     q.l1_size += (int)__popc(vm);
     if (q.l1_size > p.l1_spill) {
+        // Spill from the back; the l1_keep front (smallest-first) records stay
+        // so the warp's own chain of relaxations continues in shared memory.
         const int lane = threadIdx.x & 31;
-        for (int c = 0; c < q.l1_size; c += 32) {
+        const int first = p.l1_keep;
+        for (int c = first; c < q.l1_size; c += 32) {
             const int i = c + lane;
             const bool ok = i < q.l1_size;
             uint2 it = make_uint2(0u, 0u);
@@ -204,8 +228,8 @@ __device__ __forceinline__ void l1_write(const PlainParams &p, WarpQ &q, uint2 *
             push32(p, q, ok, it.x, it.y);
         }
         __syncwarp();
-        q.l1_head = q.l1_tail;
-        q.l1_size = 0;
+        q.l1_tail = (q.l1_head + first) & (L1_CAP - 1);
+        q.l1_size = first;
     }
 }
 
@@ -294,7 +318,10 @@ __device__ __forceinline__ int l2_read(const PlainParams &p, WarpQ &q, volatile 
 }
 
 // L3 read: only when every L2 ring is empty.  Takes up to 32 records and
-// moves `first` up to the smallest bucket among them.
+// moves `first` up to the smallest bucket among them.  Each taken record's
+// vertex bit is cleared and then the vertex's distance is read again: that
+// value covers every L3 push dropped while the record waited, and it is the
+// distance the record is relaxed with.
 __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
                                        uint2 *inb) {
     const int lane = threadIdx.x & 31;
@@ -326,9 +353,13 @@ __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile 
     if (take > ready) take = ready;
     unsigned dmin = 0xffffffffu;
     if (lane < take) {
-        inb[lane] = make_uint2(rec_v(r), rec_d(r));
+        const unsigned v = rec_v(r);
         st_relaxed64(l3_slot(p, s), SENT);
-        dmin = rec_d(r);
+        atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
+        __threadfence();
+        const unsigned cur = (unsigned)__ldcg(p.dist + v);
+        inb[lane] = make_uint2(v, cur);
+        dmin = cur;
     }
     if (take > 0) {
         for (int o = 16; o > 0; o >>= 1) dmin = min(dmin, __shfl_xor_sync(FULL, dmin, o));
@@ -358,12 +389,11 @@ struct ArcsSplit {
 
 __device__ __forceinline__ bool relax_arc(const PlainParams &p, WarpQ &q, unsigned dst,
                                           unsigned nd) {
-    const int cur = __ldcg(p.dist + dst);
     if (nd >= (unsigned)INT_MAX) {
-        if (cur == INT_MAX) q.range_hit = 1;
+        if (__ldcg(p.dist + dst) == INT_MAX) q.range_hit = 1;
         return false;
     }
-    if ((int)nd >= cur) return false;
+    if (p.precheck && (int)nd >= __ldcg(p.dist + dst)) return false;
     const int old = atomicMin(p.dist + dst, (int)nd);
     if ((int)nd < old) {
         q.improved++;

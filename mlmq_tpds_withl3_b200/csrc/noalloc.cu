@@ -12,8 +12,9 @@
 // it calls.
 //
 // Limits and behaviour (also in include/mlmq_b200.h):
-//  * workspace: 17 L2 rings of 2^17 slots + one L3 ring of 2^20 slots + the
-//    control block = MLMQ_NOALLOC_WORKSPACE_BYTES (about 26 MiB);
+//  * workspace: 17 L2 rings of 2^17 slots + one L3 ring of 2^20 slots + one
+//    L3 bit per vertex + the control block = MLMQ_NOALLOC_WORKSPACE_BYTES
+//    (about 26 MiB);
 //  * graphs up to MLMQ_NOALLOC_MAX_VERTICES vertices and MLMQ_NOALLOC_MAX_ARCS
 //    arcs, bucket_num <= 16 and at most 8 worker warps per CTA; larger
 //    requests are rejected with MLMQ_ERR_RANGE before anything runs;
@@ -44,7 +45,8 @@ constexpr int NA_WORKERS = 8;         // keeps in-flight pushes inside half a ri
 constexpr size_t NA_CTL_U64 = (ctl::WORDS + 1) / 2 + 32;  // control block, padded
 constexpr size_t NA_L2_U64 = (size_t)NA_RINGS << NA_L2_LOG;
 constexpr size_t NA_L3_U64 = (size_t)1 << NA_L3_LOG;
-constexpr size_t NA_TOTAL_U64 = NA_CTL_U64 + NA_L2_U64 + NA_L3_U64;
+constexpr size_t NA_BITS_U64 = (size_t)MLMQ_NOALLOC_MAX_VERTICES / 64;  // L3 vertex bits
+constexpr size_t NA_TOTAL_U64 = NA_CTL_U64 + NA_L2_U64 + NA_L3_U64 + NA_BITS_U64;
 static_assert(NA_TOTAL_U64 * 8 == MLMQ_NOALLOC_WORKSPACE_BYTES, "header constant out of date");
 
 // The workspace.  Host code must never pass `g_noalloc_ws` itself to a kernel
@@ -119,6 +121,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     unsigned long long *ctl_base = slot->ws;
     unsigned long long *l2 = ctl_base + NA_CTL_U64;
     unsigned long long *l3 = l2 + NA_L2_U64;
+    unsigned *l3bits = reinterpret_cast<unsigned *>(l3 + NA_L3_U64);  // cleared by the kernel
     if (!slot->clean) {
         rc = cuda_fail(cudaMemsetAsync(ctl_base, 0, NA_CTL_U64 * 8, st), "clear control");
         if (!rc) rc = cuda_fail(cudaMemsetAsync(l2, 0xff, (NA_L2_U64 + NA_L3_U64) * 8, st),
@@ -146,6 +149,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.src = src;
     p.l2 = l2;
     p.l3 = l3;
+    p.l3bits = l3bits;
     p.ctlw = reinterpret_cast<unsigned *>(ctl_base);
     p.nb = cfg.bucket_num;
     p.bm = cfg.bucket_max;
@@ -154,6 +158,8 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.large = cfg.large_degree;
     p.l1_spill = cfg.l1_spill;
     p.l1_vector = cfg.queue_type == MLMQ_L1V_L2DQ;
+    p.l1_keep = cfg.l1_keep;
+    p.precheck = cfg.relax_precheck;
     p.delta = (unsigned)cfg.delta;
     p.l2_log = NA_L2_LOG;
     p.l3_log = NA_L3_LOG;

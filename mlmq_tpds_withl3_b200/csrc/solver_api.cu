@@ -49,6 +49,20 @@ int ceil_log2(uint64_t x) {
     return l;
 }
 
+}  // namespace
+
+// L3 holds at most one record per vertex, and only reached vertices (at most
+// m + 1 of them) push: its ring gets that many slots plus room for the pushes
+// in flight, and at least 2^(MLMQ_MIN_RING_LOG2 + 1).
+int l3_ring_log2(int64_t n, int64_t m) {
+    const int64_t reach = std::min<int64_t>(n, m + 1);
+    return std::min(30, std::max(MLMQ_MIN_RING_LOG2 + 1, ceil_log2((uint64_t)reach + (1u << 16))));
+}
+
+size_t l3_bits_bytes(int64_t n) { return sizeof(unsigned) * (size_t)((n + 31) / 32); }
+
+namespace {
+
 int env_int(const char *name, int dflt, bool *present) {
     const char *s = std::getenv(name);
     if (present) *present = s != nullptr;
@@ -81,6 +95,8 @@ int validate_config(const mlmq_config &c) {
     if (c.l3_cap_log2 != 0 && (c.l3_cap_log2 < MLMQ_MIN_RING_LOG2 || c.l3_cap_log2 > 30))
         return MLMQ_ERR_ARG;
     if (c.timeout_ms < 1) return MLMQ_ERR_ARG;
+    if (c.l1_keep < 0 || c.l1_keep > c.l1_spill) return MLMQ_ERR_ARG;
+    if (c.relax_precheck != 0 && c.relax_precheck != 1) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -147,6 +163,8 @@ extern "C" int mlmq_config_default(mlmq_config *cfg) {
     cfg->l2_cap_log2 = 0;
     cfg->l3_cap_log2 = 0;
     cfg->timeout_ms = 20000;
+    cfg->l1_keep = 0;
+    cfg->relax_precheck = 1;
     int rc = MLMQ_OK;
     bool have = false;
     int d = env_int("BENCH_DELTA", 200000, &have);
@@ -262,8 +280,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
     s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
-    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2
-                                : std::min(27, std::max(MLMQ_MIN_RING_LOG2 + 1, ceil_log2(2 * m)));
+    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(g->n, g->m);
     s->workers = cfg.warps_per_block;
     int bps = 0;
     rc = cuda_fail(plain_max_blocks_per_sm(s->workers, &bps), "occupancy");
@@ -280,6 +297,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_dist, sizeof(int) * (size_t)g->n), "cudaMalloc(dist)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l2, l2_bytes), "cudaMalloc(L2)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3, l3_bytes), "cudaMalloc(L3)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(g->n)), "cudaMalloc(L3 bits)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS), "cudaMalloc(ctl)");
     if (!rc) rc = cuda_fail(cudaMallocHost(&s->h_ctl, sizeof(unsigned) * ctl::WORDS), "pinned ctl");
     if (!rc) rc = fill_device(s->d_dist, g->n, INT_MAX, s->stream);
@@ -325,6 +343,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.src = src;
     p.l2 = s->d_l2;
     p.l3 = s->d_l3;
+    p.l3bits = s->d_l3bits;
     p.ctlw = s->d_ctl;
     p.nb = s->cfg.bucket_num;
     p.bm = s->cfg.bucket_max;
@@ -333,6 +352,8 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.large = s->cfg.large_degree;
     p.l1_spill = s->cfg.l1_spill;
     p.l1_vector = s->cfg.queue_type == MLMQ_L1V_L2DQ;
+    p.l1_keep = s->cfg.l1_keep;
+    p.precheck = s->cfg.relax_precheck;
     p.delta = (unsigned)s->cfg.delta;
     p.l2_log = s->l2_log;
     p.l3_log = s->l3_log;
@@ -405,6 +426,7 @@ extern "C" void mlmq_solver_destroy(mlmq_solver *s) {
     if (s->d_dist) cudaFree(s->d_dist);
     if (s->d_l2) cudaFree(s->d_l2);
     if (s->d_l3) cudaFree(s->d_l3);
+    if (s->d_l3bits) cudaFree(s->d_l3bits);
     if (s->d_ctl) cudaFree(s->d_ctl);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->done) cudaEventDestroy(s->done);

@@ -25,6 +25,7 @@ struct mlmq_solver {
     int *d_dist = nullptr;
     unsigned long long *d_l2 = nullptr;
     unsigned long long *d_l3 = nullptr;
+    unsigned *d_l3bits = nullptr;  // one bit per vertex: the vertex has an L3 record
     unsigned *d_ctl = nullptr;
     unsigned *h_ctl = nullptr;  // pinned copy of the control block after each solve
     cudaStream_t stream = nullptr;
@@ -40,6 +41,10 @@ int fill_device(int *p, int64_t n, int v, cudaStream_t s);
 int validate_config(const mlmq_config &c);
 int status_to_error(unsigned st);
 int device_sm_count(int *sms);
+// log2 of the L3 ring size for a graph of n vertices and m arcs.
+int l3_ring_log2(int64_t n, int64_t m);
+// Bytes of the per-vertex L3 bit array.
+size_t l3_bits_bytes(int64_t n);
 
 // Reference entry points; exported with C linkage (solver_api.cu) and with the
 // reference's C++ linkage (drop_in.cpp).

@@ -53,6 +53,8 @@ struct mlmq_batch {
     int *d_dist = nullptr;            // max_q * max_n
     unsigned long long *d_l2 = nullptr;
     unsigned long long *d_l3 = nullptr;
+    unsigned *d_l3bits = nullptr;     // max_q * bits_words
+    size_t bits_words = 0;            // L3 vertex-bit words per slot
     unsigned *d_ctl = nullptr;        // max_q * CTL_STRIDE
     PlainParams *d_params = nullptr;  // max_q
     PlainParams *h_params = nullptr;  // pinned
@@ -128,7 +130,8 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     b->max_n = max_vertices;
     b->workers = cfg.warps_per_block;
     b->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : MLMQ_MIN_RING_LOG2;
-    b->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : MLMQ_MIN_RING_LOG2 + 2;
+    b->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(max_vertices, max_vertices);
+    b->bits_words = l3_bits_bytes(max_vertices) / sizeof(unsigned);
     rc = cuda_fail(cudaGetDevice(&b->device), "cudaGetDevice");
     int bps = 0;
     if (!rc) {
@@ -157,6 +160,7 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_dist, sizeof(int) * nq * (size_t)max_vertices), "batch dist");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l2, sizeof(unsigned long long) * l2_slots(b) * nq), "batch L2");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3, sizeof(unsigned long long) * (nq << b->l3_log)), "batch L3");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3bits, sizeof(unsigned) * b->bits_words * nq), "batch L3 bits");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "batch ctl");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_params, sizeof(PlainParams) * nq), "batch params");
     if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_params, sizeof(PlainParams) * nq), "pinned params");
@@ -205,6 +209,7 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         p.src = srcs[q];
         p.l2 = b->d_l2 + (size_t)q * l2s;
         p.l3 = b->d_l3 + ((size_t)q << b->l3_log);
+        p.l3bits = b->d_l3bits + (size_t)q * b->bits_words;
         p.ctlw = b->d_ctl + (size_t)q * CTL_STRIDE;
         p.nb = b->cfg.bucket_num;
         p.bm = b->cfg.bucket_max;
@@ -213,6 +218,8 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         p.large = b->cfg.large_degree;
         p.l1_spill = b->cfg.l1_spill;
         p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
+        p.l1_keep = b->cfg.l1_keep;
+        p.precheck = b->cfg.relax_precheck;
         p.delta = (unsigned)b->cfg.delta;
         p.l2_log = b->l2_log;
         p.l3_log = b->l3_log;
@@ -323,6 +330,7 @@ extern "C" void mlmq_batch_destroy(mlmq_batch *b) {
     cudaFree(b->d_dist);
     cudaFree(b->d_l2);
     cudaFree(b->d_l3);
+    cudaFree(b->d_l3bits);
     cudaFree(b->d_ctl);
     cudaFree(b->d_params);
     if (b->h_params) cudaFreeHost(b->h_params);

@@ -9,7 +9,8 @@
 // guarantees all CTAs are resident, so the in-kernel barriers and the
 // manager/worker hand-offs cannot wait on a CTA that never started.
 //
-// Prologue: fill dist with INT_MAX, reset the queue counters, barrier, seed
+// Prologue: fill dist with INT_MAX, clear the L3 vertex bits, reset the queue
+// counters, barrier, seed
 // the source record into bucket 0, barrier.  Then workers loop
 // L1 -> L2 window -> L3 -> relax, and manager warps mirror the counters into
 // shared memory; CTA 0's manager also detects termination and moves `first`.
@@ -154,6 +155,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     const size_t gtid = (size_t)grank * blockDim.x + threadIdx.x;
     const size_t gstride = (size_t)gsize * blockDim.x;
     for (size_t i = gtid; i < (size_t)p.n; i += gstride) p.dist[i] = INT_MAX;
+    for (size_t i = gtid; i < ((size_t)p.n + 31) / 32; i += gstride) p.l3bits[i] = 0u;
     if (grank == 0) {
         for (int i = threadIdx.x; i < ctl::WORDS; i += blockDim.x)
             if (i != ctl::BAR_COUNT && i != ctl::BAR_GEN) p.ctlw[i] = 0u;

@@ -74,6 +74,8 @@ struct ServerParams {
     volatile unsigned *shutdown;  // mapped
     int *dist;                    // slots * max_n
     unsigned long long *l2, *l3;
+    unsigned *l3bits;             // slots * bits_words
+    size_t bits_words;
     unsigned *ctl;                // slots * SRV_CTL_STRIDE
     int slots, max_n;
     unsigned long long lifetime_ns;
@@ -180,6 +182,7 @@ __global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
         p.dist = sp.dist + (size_t)s * sp.max_n;
         p.l2 = sp.l2 + ((size_t)s * (p.nb + 1) << p.l2_log);
         p.l3 = sp.l3 + ((size_t)s << p.l3_log);
+        p.l3bits = sp.l3bits + (size_t)s * sp.bits_words;
         p.ctlw = c;
         plain_body<ArcsInterleaved>(p, grank, gsize);
         // A solve that stopped early leaves records in the rings: the group
@@ -225,6 +228,8 @@ struct mlmq_server {
     int slots = 0, max_n = 0, grid = 0, workers = 0, l2_log = 0, l3_log = 0;
     int *d_dist = nullptr;
     unsigned long long *d_l2 = nullptr, *d_l3 = nullptr;
+    unsigned *d_l3bits = nullptr;
+    size_t bits_words = 0;
     unsigned *d_ctl = nullptr;
     SlotCommand *h_cmd = nullptr;
     SlotCompletion *h_done = nullptr;
@@ -267,13 +272,14 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
     sv->cfg = cfg;
     sv->workers = cfg.warps_per_block;
     sv->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2 : MLMQ_MIN_RING_LOG2;
-    sv->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : MLMQ_MIN_RING_LOG2 + 2;
+    sv->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(max_vertices, max_vertices);
+    sv->bits_words = l3_bits_bytes(max_vertices) / sizeof(unsigned);
     sv->max_n = max_vertices;
     rc = cuda_fail(cudaGetDevice(&sv->device), "cudaGetDevice");
     // Admission by free device memory: as many slots as fit after a reserve.
     const size_t per_slot = sizeof(int) * (size_t)max_vertices +
                             8 * (((size_t)(cfg.bucket_num + 1) << sv->l2_log) + ((size_t)1 << sv->l3_log)) +
-                            4 * SRV_CTL_STRIDE;
+                            4 * SRV_CTL_STRIDE + 4 * sv->bits_words;
     size_t free_b = 0, total_b = 0;
     if (!rc) rc = cuda_fail(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
     if (!rc) {
@@ -299,6 +305,7 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_dist, sizeof(int) * ns * (size_t)max_vertices), "server dist");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l2, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log)), "server L2");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3, 8 * (ns << sv->l3_log)), "server L3");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3bits, 4 * ns * sv->bits_words), "server L3 bits");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_ctl, 4 * ns * SRV_CTL_STRIDE), "server ctl");
     if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_cmd, sizeof(SlotCommand) * ns, cudaHostAllocMapped), "cmd");
     if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_done, sizeof(SlotCompletion) * ns, cudaHostAllocMapped), "done");
@@ -327,6 +334,8 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         b.large = cfg.large_degree;
         b.l1_spill = cfg.l1_spill;
         b.l1_vector = cfg.queue_type == MLMQ_L1V_L2DQ;
+        b.l1_keep = cfg.l1_keep;
+        b.precheck = cfg.relax_precheck;
         b.delta = (unsigned)cfg.delta;
         b.l2_log = sv->l2_log;
         b.l3_log = sv->l3_log;
@@ -342,6 +351,8 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         sp.dist = sv->d_dist;
         sp.l2 = sv->d_l2;
         sp.l3 = sv->d_l3;
+        sp.l3bits = sv->d_l3bits;
+        sp.bits_words = sv->bits_words;
         sp.ctl = sv->d_ctl;
         sp.slots = sv->slots;
         sp.max_n = max_vertices;
@@ -479,6 +490,7 @@ extern "C" void mlmq_server_destroy(mlmq_server *sv) {
     cudaFree(sv->d_dist);
     cudaFree(sv->d_l2);
     cudaFree(sv->d_l3);
+    cudaFree(sv->d_l3bits);
     cudaFree(sv->d_ctl);
     if (sv->h_cmd) cudaFreeHost(sv->h_cmd);
     if (sv->h_done) cudaFreeHost(sv->h_done);

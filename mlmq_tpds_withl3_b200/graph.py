@@ -101,6 +101,35 @@ class HostGraph:
     def write_gr(self, path):
         check(lib.mlmq_hgraph_write_gr(self._h, os.fsencode(path)), f"write {path}")
 
+    # ---- transforms ----------------------------------------------------------
+    def reorder_bfs(self, root=0):
+        """BFS locality order (reference graph_transform/reorder_gr.cu:96-190).
+
+        Returns (graph, perm, invperm): new ids follow the discovery order of
+        a queue BFS from ``root`` that scans arcs in CSR order, unreached
+        vertices follow in ascending id; perm[new] = old, invperm[old] = new.
+        Distances carry over as dist_new[invperm[v]] == dist_old[v]."""
+        h = ctypes.c_void_p()
+        perm = np.empty(self.n, dtype=np.int32)
+        inv = np.empty(self.n, dtype=np.int32)
+        check(lib.mlmq_hgraph_reorder_bfs(self._h, int(root), ctypes.byref(h), perm.ctypes.data,
+                                          inv.ctypes.data), "mlmq_hgraph_reorder_bfs")
+        return HostGraph(h.value, f"{self.name}.bfs{root}"), perm, inv
+
+    def chain_shortcuts(self, source=0, cut=None):
+        """Chain-shortcut augmentation G+ (reference
+        SSSP/l3/l3_chain_shortcuts.h:23-109): one extra arc per maximal walk
+        through degree-2 chain vertices, every original arc kept, so all
+        shortest-path distances are unchanged.  ``cut`` = n (default) places
+        no partition restriction.  Returns (graph, stats)."""
+        cut = self.n if cut is None else int(cut)
+        h = ctypes.c_void_p()
+        st = np.zeros(5, dtype=np.int64)
+        check(lib.mlmq_hgraph_chain_shortcuts(self._h, cut, int(source), ctypes.byref(h),
+                                              st.ctypes.data), "mlmq_hgraph_chain_shortcuts")
+        keys = ("chain_vertices", "shortcuts", "longest_walk", "overflow_walks", "arcs_replaced")
+        return HostGraph(h.value, f"{self.name}+"), dict(zip(keys, (int(x) for x in st)))
+
     # ---- statistics ----------------------------------------------------------
     def info(self):
         """The reference's graph_info (core/include/graph_info.h:24-67):

@@ -107,3 +107,50 @@ def ref_sequential(g, src):
     if rc:
         raise RuntimeError(f"ref_sssp_sequential rc={rc}")
     return d, work.value
+
+
+CHAIN_SO = os.path.join(ROOT, "oracle", "_ref", "libref_chain.so")
+REORDER_BIN = os.path.join(ROOT, "oracle", "_ref", "reorder_gr")
+
+
+def ref_chain_shortcuts(g, source, cut=None):
+    """The reference's own chain-shortcut builder (SSSP/l3/l3_chain_shortcuts.h,
+    compiled into oracle/_ref/libref_chain.so) -> (row, col, w, stats[5]), or
+    None when that checker was not built."""
+    if not os.path.exists(CHAIN_SO):
+        return None
+    lib = ctypes.CDLL(CHAIN_SO)
+    lib.ref_chain_shortcuts.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
+                                        ctypes.c_int, _vp, _vp, _vp, ctypes.c_longlong,
+                                        ctypes.POINTER(ctypes.c_longlong), _vp]
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    cut = n if cut is None else cut
+    cap = 2 * len(col) + 1
+    orow = np.empty(n + 1, np.int32)
+    ocol = np.empty(cap, np.int32)
+    ow = np.empty(cap, np.int32)
+    om = ctypes.c_longlong()
+    st = np.zeros(5, np.int64)
+    rc = lib.ref_chain_shortcuts(n, len(col), row.ctypes.data, col.ctypes.data, w.ctypes.data,
+                                 int(cut), int(source), orow.ctypes.data, ocol.ctypes.data,
+                                 ow.ctypes.data, cap, ctypes.byref(om), st.ctypes.data)
+    if rc:
+        raise RuntimeError(f"ref_chain_shortcuts rc={rc}")
+    return orow, ocol[:om.value].copy(), ow[:om.value].copy(), st
+
+
+def ref_reorder_bfs(gr_path, root, workdir):
+    """Runs the reference's reorder_gr tool (oracle/_ref/reorder_gr) on a .gr
+    file -> (out .gr path, perm, invperm), or None when it was not built."""
+    if not os.path.exists(REORDER_BIN):
+        return None
+    import subprocess
+    out = os.path.join(workdir, "reordered.gr")
+    res = subprocess.run([REORDER_BIN, gr_path, out, str(int(root))], capture_output=True,
+                         text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"reorder_gr failed: {res.stdout}{res.stderr}")
+    perm = np.fromfile(out + ".perm.u32", dtype="<u4").astype(np.int32)
+    inv = np.fromfile(out + ".invperm.u32", dtype="<u4").astype(np.int32)
+    return out, perm, inv

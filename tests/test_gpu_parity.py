@@ -70,6 +70,9 @@ def test_c1_grid512_bit_exact():
     {"large_degree": 1},
     {"l1_spill": 1},
     {"l2_cap_log2": 18, "l3_cap_log2": 18},
+    {"l1_keep": 8},
+    {"l1_keep": 32, "queue_type": MLMQ_L1V_L2DQ},
+    {"relax_precheck": 0},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
@@ -108,6 +111,33 @@ def test_l2_pressure_path_exact():
                                         "delta": 1 << 30, "l1_spill": 1,
                                         "timeout_ms": 10000})
     assert np.array_equal(s.solve(1).dist(), ref)
+
+
+def test_l3_one_record_per_vertex_bounds_the_ring():
+    """Narrow buckets over a two-bucket window send most pushes of an R-MAT
+    graph to L3, whose ring (2^19 slots) is smaller than the pushes it sees:
+    L3 keeps one record per vertex (n = 2^18), so the ring never fills and
+    the result stays exact."""
+    g = HostGraph.rmat(18, seed=12)
+    ref, _ = oracle_lib.sssp_i32(g, 0)
+    s = Solver(DeviceGraph.upload(g), {"bucket_num": 2, "bucket_max": 1, "delta": 2000,
+                                        "l3_cap_log2": 19, "timeout_ms": 15000})
+    assert np.array_equal(s.solve(0).dist(), ref)
+    assert s.stats()["l3_pushed"] > 0
+
+
+def test_transformed_graphs_solve_exact():
+    """G+ (chain shortcuts) and the BFS-reordered graph on the GPU: the same
+    distances as the original graph, permuted for the reordering."""
+    g = HostGraph.grid(256, 256, drop_p=0.25, seed=31)
+    src = 123
+    ref, _ = oracle_lib.sssp_i32(g, src)
+    gp, st = g.chain_shortcuts(source=src)
+    assert st["shortcuts"] > 0
+    assert np.array_equal(Solver(DeviceGraph.upload(gp)).solve(src).dist(), ref)
+    r, perm, inv = g.reorder_bfs(src)
+    got = Solver(DeviceGraph.upload(r)).solve(int(inv[src])).dist()
+    assert np.array_equal(got[inv], ref)
 
 
 def test_timeout_is_reported_not_hung():
