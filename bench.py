@@ -488,7 +488,7 @@ def run_served(args):
         sched = poisson_schedule(rate, count, ns, seed=100 + ri)
         keep = (lambda i: i % 40 == 0)
         recs = serve_poisson(sv, dgs, sched, keep=keep, pool=pool, timeout_s=600)
-        s = summarize(recs)
+        s = summarize(recs, names)
         s["rate"] = rate
         sweep.append(s)
         for i, r in enumerate(recs):
@@ -500,6 +500,7 @@ def run_served(args):
     solvers = {}
     correct = True
     plain_ms = []
+    plain_by_graph = {}
     stream = torch.cuda.Stream()
     for (ri, i), r in sample.items():
         gi = r["graph"]
@@ -513,7 +514,8 @@ def run_served(args):
         e1.record(stream)
         s.wait()
         plain_ms.append(e0.elapsed_time(e1))
-        if not np.array_equal(s.dist(), r["dist"]):
+        plain_by_graph.setdefault(names[gi], []).append(plain_ms[-1])
+        if r["status"] or not np.array_equal(s.dist(), r["dist"]):
             correct = False
     for s in solvers.values():
         s.close()
@@ -531,7 +533,9 @@ def run_served(args):
         "sweep": sweep,
         "latency_ms": {"p50": top["p50_ms"], "p99": top["p99_ms"], "at_rate": top["rate"]},
         "plain_back_to_back": {"qps": plain_qps, "queries": len(plain_ms),
-                               "ms_per_query_mean": float(np.mean(plain_ms))},
+                               "ms_per_query_mean": float(np.mean(plain_ms)),
+                               "ms_mean_by_graph": {k: float(np.mean(v))
+                                                    for k, v in sorted(plain_by_graph.items())}},
         "speedup_vs_plain_qps": top["qps"] / plain_qps,
         "correct": bool(correct),
         "checked_alone_vs_mix": len(sample),

@@ -19,6 +19,7 @@ constexpr int FIRST = 0;      // current first bucket (absolute index)
 constexpr int EXIT = 1;       // 1 = all warps leave the persistent loop
 constexpr int STATUS = 2;     // ST_* bits
 constexpr int PRESSURE = 3;   // bit b: L2 bucket b is filling, new pushes go to L3
+constexpr int U_PRESSURE = 4; // 1: the urgent ring is filling, its pushes go to L3
 constexpr int BAR_COUNT = 8;  // grid barrier arrivals (self-resetting)
 constexpr int BAR_GEN = 9;    // grid barrier generation
 constexpr int CREDIT = 32;    // records read from L2/L3 whose work is finished

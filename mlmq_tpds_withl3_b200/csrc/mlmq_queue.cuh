@@ -132,11 +132,12 @@ __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool vali
     const int lane = threadIdx.x & 31;
     const unsigned f = ld_relaxed(p.ctlw + ctl::FIRST);
     const unsigned pres = ld_relaxed(p.ctlw + ctl::PRESSURE);
+    const unsigned upres = ld_relaxed(p.ctlw + ctl::U_PRESSURE);
     int tgt = -1;
     if (valid) {
         const unsigned L = d / p.delta;
         if (L < f) {
-            tgt = p.nb;  // urgent ring
+            tgt = upres ? NB_MAX : p.nb;  // urgent ring, or L3 while it is filling
         } else if (L - f >= (unsigned)p.nb) {
             tgt = NB_MAX;  // L3
         } else {
@@ -167,8 +168,15 @@ __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool vali
         if (tgt < NB_MAX) {
             const unsigned cons = ld_relaxed(p.ctlw + ctl::CONSUMED + tgt);
             base = atomicAdd(p.ctlw + ctl::RESERVE + tgt, cnt);
-            if (base + cnt - cons > (1u << (p.l2_log - 1)) && tgt < p.nb)
-                atomicOr(p.ctlw + ctl::PRESSURE, 1u << tgt);
+            // More than half the ring outstanding: later pushes for this ring
+            // go to L3 until it drains.  The urgent ring needs this as much
+            // as a bucket: every record produced below the window goes
+            // there, and a full ring would leave pushers waiting for slots
+            // that only other (pushing) warps can free.
+            if (base + cnt - cons > (1u << (p.l2_log - 1))) {
+                if (tgt < p.nb) atomicOr(p.ctlw + ctl::PRESSURE, 1u << tgt);
+                else st_relaxed(p.ctlw + ctl::U_PRESSURE, 1u);
+            }
         } else {
             base = atomicAdd(p.ctlw + ctl::L3_RESERVE, cnt);
         }

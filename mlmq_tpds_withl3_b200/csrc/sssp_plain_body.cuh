@@ -83,6 +83,8 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
                 // Release bucket pressure once the ring has drained.
                 if (lane < p.nb && ((pres >> lane) & 1u) && res - con < cap8)
                     atomicAnd(p.ctlw + ctl::PRESSURE, ~(1u << lane));
+                if (lane == p.nb && res - con < cap8 && ld_relaxed(p.ctlw + ctl::U_PRESSURE))
+                    st_relaxed(p.ctlw + ctl::U_PRESSURE, 0u);
             }
         }
         if (!ex && globaltimer() > deadline) {

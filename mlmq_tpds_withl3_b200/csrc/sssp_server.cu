@@ -204,6 +204,9 @@ __global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
         if (grank == 0 && threadIdx.x == 0) {
             const unsigned long long *u = reinterpret_cast<const unsigned long long *>(c + ctl::STATS);
             unsigned st = ld_acquire(c + ctl::STATUS);
+            // A grid barrier of the solve that gave up left its arrival count
+            // behind; no CTA of the slot is inside the solve now.
+            if (st & ST_TIMEOUT) st_relaxed(c + ctl::BAR_COUNT, 0u);
             if (!ok) st |= ST_TIMEOUT;
             sp.done[s].status = st;
             sp.done[s].first_max = (unsigned)u[ctl::ST_FIRST_MAX];

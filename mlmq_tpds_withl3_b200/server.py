@@ -135,9 +135,28 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
     return out
 
 
-def summarize(records):
+def summarize(records, names=None):
+    """Throughput, latency percentiles and error counts of a served run;
+    with `names` (graph index -> name) also per graph."""
     lat = np.array([r["latency_s"] for r in records]) * 1e3
     span = max(r["finish"] for r in records) - min(r["arrival"] for r in records)
-    return {"queries": len(records), "qps": len(records) / span,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "errors": sum(1 for r in records if r["status"])}
+    codes = {}
+    for r in records:
+        if r["status"]:
+            codes[str(r["status"])] = codes.get(str(r["status"]), 0) + 1
+    out = {"queries": len(records), "qps": len(records) / span,
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "mean_ms": float(lat.mean()), "errors": sum(codes.values()), "error_codes": codes}
+    if names is not None:
+        per = {}
+        for gi, name in enumerate(names):
+            sel = [r for r in records if r["graph"] == gi]
+            if not sel:
+                continue
+            run = np.array([r["finish"] - r["start"] for r in sel]) * 1e3
+            gl = np.array([r["latency_s"] for r in sel]) * 1e3
+            per[name] = {"queries": len(sel), "errors": sum(1 for r in sel if r["status"]),
+                         "p50_ms": float(np.percentile(gl, 50)),
+                         "run_ms_mean": float(run.mean())}
+        out["per_graph"] = per
+    return out
