@@ -62,6 +62,9 @@ const char *mlmq_strerror(int code);
 
 /* Smallest queue ring (log2 slots) a configuration may ask for. */
 #define MLMQ_MIN_RING_LOG2 18
+/* Most worker warps per CTA when relax_unroll > 1 (plus one manager warp:
+   800 threads); with relax_unroll 1 the limit is 31. */
+#define MLMQ_MAX_UNROLLED_WARPS 24
 
 typedef struct mlmq_config {
     int queue_type;      /* MLMQ_L1SLF_L2DQ (default) or MLMQ_L1V_L2DQ */
@@ -85,6 +88,9 @@ typedef struct mlmq_config {
                             all, the reference's rule; at most l1_spill) */
     int relax_precheck;  /* 1: read dist[dst] before atomicMin (default);
                             0: atomicMin directly (one less dependent load) */
+    int relax_unroll;    /* rounds of 32 arcs a warp keeps in flight: 1, 2 or
+                            4 (default 4; above 1 at most
+                            MLMQ_MAX_UNROLLED_WARPS worker warps per CTA) */
 } mlmq_config;
 
 /* Fills *cfg with the reference's defaults (common.h:24-34, sssp.cuh:20,

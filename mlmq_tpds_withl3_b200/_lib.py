@@ -60,7 +60,8 @@ class Config(ctypes.Structure):
     _fields_ = [(n, c_int) for n in (
         "queue_type", "delta", "work_blocks", "warps_per_block", "l2_batch",
         "bucket_num", "bucket_max", "min_read", "large_degree", "l1_spill",
-        "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck")]
+        "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck",
+        "relax_unroll")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -75,7 +75,8 @@ def _time_solve(solver, src, reps=2):
 def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
          extra=None):
     """Returns (config, report).  Candidates: delta from delta_candidates(),
-    then warps per CTA in {8, 16, 24} at the best delta."""
+    then warps per CTA in {8, 16, 24} at the best delta, then 1, 2 or 4
+    relaxation rounds in flight."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -100,6 +101,12 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
     best_t = min(r["seconds"] for r in results if r["config"] == best)
     for wpb in (8, 24):
         over = {"delta": best_d, "warps_per_block": wpb}
+        t = measure(over)
+        if t < best_t:
+            best, best_t = over, t
+    # Relaxation rounds in flight per warp (default 4) at the best shape.
+    for unroll in (1, 2):
+        over = {**best, "relax_unroll": unroll}
         t = measure(over)
         if t < best_t:
             best, best_t = over, t

@@ -395,23 +395,56 @@ struct ArcsSplit {
     }
 };
 
-__device__ __forceinline__ bool relax_arc(const PlainParams &p, WarpQ &q, unsigned dst,
-                                          unsigned nd) {
-    if (nd >= (unsigned)INT_MAX) {
-        if (__ldcg(p.dist + dst) == INT_MAX) q.range_hit = 1;
-        return false;
+// Relaxes up to K rounds of 32 arcs (lane-distributed: round k gives this lane
+// arc ai[k] of a vertex at distance du[k] when ok[k]) and feeds the winners to
+// L1.  The rounds' arc loads, then their destination-distance loads, then
+// their atomicMins are issued back to back, so a warp keeps K independent
+// dependent-load chains in flight instead of one; `rounds` (warp-uniform) is
+// the number of rounds that hold any arc.
+template <class Arcs, int K>
+__device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uint2 *ring,
+                                             const bool (&ok)[K], const int (&ai)[K],
+                                             const unsigned (&du)[K], int rounds) {
+    unsigned dst[K], nd[K];
+    int cur[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        dst[k] = 0u;
+        nd[k] = 0u;
+        if (ok[k]) {
+            const int2 a = Arcs::load(p, ai[k]);
+            dst[k] = (unsigned)a.x;
+            nd[k] = du[k] + (unsigned)a.y;
+        }
     }
-    if (p.precheck && (int)nd >= __ldcg(p.dist + dst)) return false;
-    const int old = atomicMin(p.dist + dst, (int)nd);
-    if ((int)nd < old) {
-        q.improved++;
-        return true;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        cur[k] = INT_MAX;
+        if (ok[k] && (p.precheck || nd[k] >= (unsigned)INT_MAX)) cur[k] = __ldcg(p.dist + dst[k]);
     }
-    return false;
+    bool win[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        win[k] = false;
+        if (ok[k]) {
+            if (nd[k] >= (unsigned)INT_MAX) {
+                if (cur[k] == INT_MAX) q.range_hit = 1;  // a finite distance would not fit
+            } else if ((int)nd[k] < cur[k]) {
+                win[k] = (int)nd[k] < atomicMin(p.dist + dst[k], (int)nd[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        if (k < rounds) {
+            q.improved += win[k];
+            l1_write(p, q, ring, win[k], dst[k], nd[k]);
+        }
+    }
 }
 
 // Relaxes up to 32 records (one per lane) and feeds the winners to L1.
-template <class Arcs>
+template <class Arcs, int K>
 __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
                                             unsigned v, unsigned d) {
     const int lane = threadIdx.x & 31;
@@ -438,17 +471,18 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         const int lb = __shfl_sync(FULL, beg, sl);
         const int ld = __shfl_sync(FULL, deg, sl);
         const unsigned lu = __shfl_sync(FULL, du, sl);
-        for (int e0 = 0; e0 < ld; e0 += 32) {
-            const int e = e0 + lane;
-            bool win = false;
-            unsigned dst = 0, nd = 0;
-            if (e < ld) {
-                const int2 a = Arcs::load(p, lb + e);
-                dst = (unsigned)a.x;
-                nd = lu + (unsigned)a.y;
-                win = relax_arc(p, q, dst, nd);
+        for (int e0 = 0; e0 < ld; e0 += 32 * K) {
+            bool ok[K];
+            int ai[K];
+            unsigned uu[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int e = e0 + 32 * k + lane;
+                ok[k] = e < ld;
+                ai[k] = lb + e;
+                uu[k] = lu;
             }
-            l1_write(p, q, ring, win, dst, nd);
+            relax_rounds<Arcs, K>(p, q, ring, ok, ai, uu, (ld - e0 + 31) >> 5);
         }
     }
     if (deg >= p.large) deg = 0;
@@ -463,26 +497,26 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
     }
     const int total = __shfl_sync(FULL, incl, 31);
     const int off = incl - deg;
-    for (int e0 = 0; e0 < total; e0 += 32) {
-        const int e = e0 + lane;
-        int j = 0;
+    for (int e0 = 0; e0 < total; e0 += 32 * K) {
+        bool ok[K];
+        int ai[K];
+        unsigned uu[K];
 #pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-            const int oc = __shfl_sync(FULL, off, j + s);
-            if (oc <= e) j += s;
+        for (int k = 0; k < K; k++) {
+            const int e = e0 + 32 * k + lane;
+            int j = 0;
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) {
+                const int oc = __shfl_sync(FULL, off, j + s);
+                if (oc <= e) j += s;
+            }
+            const int ob = __shfl_sync(FULL, beg, j);
+            const int oo = __shfl_sync(FULL, off, j);
+            uu[k] = __shfl_sync(FULL, du, j);
+            ok[k] = e < total;
+            ai[k] = ob + (e - oo);
         }
-        const int ob = __shfl_sync(FULL, beg, j);
-        const int oo = __shfl_sync(FULL, off, j);
-        const unsigned ou = __shfl_sync(FULL, du, j);
-        bool win = false;
-        unsigned dst = 0, nd = 0;
-        if (e < total) {
-            const int2 a = Arcs::load(p, ob + (e - oo));
-            dst = (unsigned)a.x;
-            nd = ou + (unsigned)a.y;
-            win = relax_arc(p, q, dst, nd);
-        }
-        l1_write(p, q, ring, win, dst, nd);
+        relax_rounds<Arcs, K>(p, q, ring, ok, ai, uu, (total - e0 + 31) >> 5);
     }
 }
 

@@ -54,8 +54,9 @@ static_assert(NA_TOTAL_U64 * 8 == MLMQ_NOALLOC_WORKSPACE_BYTES, "header constant
 // device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned long long g_noalloc_ws[NA_TOTAL_U64];
 
+// Relaxes one round of 32 arcs at a time (relax_unroll does not apply here).
 __global__ void __launch_bounds__(1024, 1) sssp_noalloc_kernel(PlainParams p) {
-    plain_body<ArcsSplit>(p, blockIdx.x, gridDim.x);
+    plain_body<ArcsSplit, 1>(p, blockIdx.x, gridDim.x);
 }
 
 struct DeviceSlot {

@@ -97,6 +97,8 @@ int validate_config(const mlmq_config &c) {
     if (c.timeout_ms < 1) return MLMQ_ERR_ARG;
     if (c.l1_keep < 0 || c.l1_keep > c.l1_spill) return MLMQ_ERR_ARG;
     if (c.relax_precheck != 0 && c.relax_precheck != 1) return MLMQ_ERR_ARG;
+    if (c.relax_unroll != 1 && c.relax_unroll != 2 && c.relax_unroll != 4) return MLMQ_ERR_ARG;
+    if (c.relax_unroll > 1 && c.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -165,6 +167,7 @@ extern "C" int mlmq_config_default(mlmq_config *cfg) {
     cfg->timeout_ms = 20000;
     cfg->l1_keep = 0;
     cfg->relax_precheck = 1;
+    cfg->relax_unroll = 4;
     int rc = MLMQ_OK;
     bool have = false;
     int d = env_int("BENCH_DELTA", 200000, &have);
@@ -283,7 +286,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(g->n, g->m);
     s->workers = cfg.warps_per_block;
     int bps = 0;
-    rc = cuda_fail(plain_max_blocks_per_sm(s->workers, &bps), "occupancy");
+    rc = cuda_fail(plain_max_blocks_per_sm(s->workers, cfg.relax_unroll, &bps), "occupancy");
     if (!rc && bps < 1) rc = MLMQ_ERR_UNSUPPORTED;
     if (!rc) {
         const int maxgrid = bps * sms;
@@ -359,7 +362,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.l3_log = s->l3_log;
     p.workers = s->workers;
     p.timeout_ns = (unsigned long long)s->cfg.timeout_ms * 1000000ull;
-    rc = cuda_fail(plain_launch(p, s->grid, st), "persistent launch");
+    rc = cuda_fail(plain_launch(p, s->cfg.relax_unroll, s->grid, st), "persistent launch");
     if (rc) {
         s->dirty = true;
         return rc;

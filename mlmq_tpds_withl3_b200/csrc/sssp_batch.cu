@@ -30,15 +30,50 @@ namespace mlmq {
 
 constexpr int CTL_STRIDE = 512;  // words per slot control block (2 KiB, padded)
 
-__global__ void __launch_bounds__(1024, 1) sssp_batch_kernel(const PlainParams *__restrict__ slots,
-                                                             int nq) {
+// What differs between the queries of a launch; everything else (queue
+// configuration, per-slot workspace strides) is one kernel parameter, so it
+// stays in the constant bank instead of occupying registers.
+struct BatchQuery {
+    const int *row;
+    const int2 *arcs;
+    int n, src;
+};
+struct BatchParams {
+    PlainParams base;  // configuration; dist/l2/l3/l3bits/ctlw point at slot 0's arrays
+    const BatchQuery *__restrict__ queries;
+    size_t dist_stride, l2_stride, l3_stride, bits_stride, ctl_stride;
+    int nq;
+};
+
+template <int K>
+__global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
+    sssp_batch_kernel(BatchParams bp) {
     const unsigned g = gridDim.x;
-    const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)nq) / g);
+    const unsigned nq = (unsigned)bp.nq;
+    const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * nq) / g);
     // First CTA of slot s: ceil(s * g / nq).
-    const unsigned lo = (unsigned)(((unsigned long long)s * g + nq - 1) / (unsigned)nq);
-    const unsigned hi = (unsigned)(((unsigned long long)(s + 1) * g + nq - 1) / (unsigned)nq);
-    const PlainParams p = slots[s];
-    plain_body<ArcsInterleaved>(p, blockIdx.x - lo, hi - lo);
+    const unsigned lo = (unsigned)(((unsigned long long)s * g + nq - 1) / nq);
+    const unsigned hi = (unsigned)(((unsigned long long)(s + 1) * g + nq - 1) / nq);
+    PlainParams p = bp.base;
+    const BatchQuery qy = bp.queries[s];
+    p.row = qy.row;
+    p.arcs = qy.arcs;
+    p.n = qy.n;
+    p.src = qy.src;
+    p.dist = bp.base.dist + s * bp.dist_stride;
+    p.l2 = bp.base.l2 + s * bp.l2_stride;
+    p.l3 = bp.base.l3 + s * bp.l3_stride;
+    p.l3bits = bp.base.l3bits + s * bp.bits_stride;
+    p.ctlw = bp.base.ctlw + s * bp.ctl_stride;
+    plain_body<ArcsInterleaved, K>(p, blockIdx.x - lo, hi - lo);
+}
+
+const void *batch_kernel(int unroll) {
+    switch (unroll) {
+        case 1: return (const void *)sssp_batch_kernel<1>;
+        case 2: return (const void *)sssp_batch_kernel<2>;
+        default: return (const void *)sssp_batch_kernel<4>;
+    }
 }
 
 }  // namespace mlmq
@@ -56,8 +91,8 @@ struct mlmq_batch {
     unsigned *d_l3bits = nullptr;     // max_q * bits_words
     size_t bits_words = 0;            // L3 vertex-bit words per slot
     unsigned *d_ctl = nullptr;        // max_q * CTL_STRIDE
-    PlainParams *d_params = nullptr;  // max_q
-    PlainParams *h_params = nullptr;  // pinned
+    BatchQuery *d_queries = nullptr;  // max_q
+    BatchQuery *h_queries = nullptr;  // pinned
     unsigned *h_ctl = nullptr;        // pinned copy of the control blocks
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -88,8 +123,8 @@ int reset_all(mlmq_batch *b, cudaStream_t st) {
 int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     const int threads = 32 * (b->workers + 1);
     const size_t smem = plain_smem_bytes(b->workers);
-    int rc = cuda_fail(cudaMemcpyAsync(b->d_params, b->h_params, sizeof(PlainParams) * nq,
-                                       cudaMemcpyHostToDevice, st), "batch params");
+    int rc = cuda_fail(cudaMemcpyAsync(b->d_queries, b->h_queries, sizeof(BatchQuery) * nq,
+                                       cudaMemcpyHostToDevice, st), "batch queries");
     if (rc) return rc;
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)b->grid);
@@ -101,8 +136,37 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     attr[0].val.cooperative = 1;
     lc.attrs = attr;
     lc.numAttrs = b->graph_cooperative ? 1 : 0;
-    const PlainParams *params = b->d_params;
-    rc = cuda_fail(cudaLaunchKernelEx(&lc, sssp_batch_kernel, params, nq), "batch launch");
+    BatchParams bp{};
+    PlainParams &p = bp.base;
+    p.dist = b->d_dist;
+    p.l2 = b->d_l2;
+    p.l3 = b->d_l3;
+    p.l3bits = b->d_l3bits;
+    p.ctlw = b->d_ctl;
+    p.nb = b->cfg.bucket_num;
+    p.bm = b->cfg.bucket_max;
+    p.batch = b->cfg.l2_batch;
+    p.min_read = b->cfg.min_read;
+    p.large = b->cfg.large_degree;
+    p.l1_spill = b->cfg.l1_spill;
+    p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
+    p.l1_keep = b->cfg.l1_keep;
+    p.precheck = b->cfg.relax_precheck;
+    p.delta = (unsigned)b->cfg.delta;
+    p.l2_log = b->l2_log;
+    p.l3_log = b->l3_log;
+    p.workers = b->workers;
+    p.timeout_ns = (unsigned long long)b->cfg.timeout_ms * 1000000ull;
+    bp.queries = b->d_queries;
+    bp.dist_stride = (size_t)b->max_n;
+    bp.l2_stride = l2_slots(b);
+    bp.l3_stride = (size_t)1 << b->l3_log;
+    bp.bits_stride = b->bits_words;
+    bp.ctl_stride = CTL_STRIDE;
+    bp.nq = nq;
+    void *args[] = {&bp};
+    rc = cuda_fail(cudaLaunchKernelExC(&lc, batch_kernel(b->cfg.relax_unroll), args),
+                   "batch launch");
     if (rc) return rc;
     return cuda_fail(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq,
                                      cudaMemcpyDeviceToHost, st), "batch status");
@@ -137,12 +201,11 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     if (!rc) {
         const int threads = 32 * (b->workers + 1);
         const size_t smem = plain_smem_bytes(b->workers);
-        rc = cuda_fail(cudaFuncSetAttribute(sssp_batch_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                       "batch smem");
+        const void *k = batch_kernel(cfg.relax_unroll);
+        rc = cuda_fail(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem), "batch smem");
         if (!rc)
-            rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_batch_kernel,
-                                                                         threads, smem),
+            rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem),
                            "batch occupancy");
     }
     if (!rc) {
@@ -162,8 +225,8 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3, sizeof(unsigned long long) * (nq << b->l3_log)), "batch L3");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3bits, sizeof(unsigned) * b->bits_words * nq), "batch L3 bits");
     if (!rc) rc = cuda_fail(cudaMalloc(&b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "batch ctl");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_params, sizeof(PlainParams) * nq), "batch params");
-    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_params, sizeof(PlainParams) * nq), "pinned params");
+    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_queries, sizeof(BatchQuery) * nq), "batch queries");
+    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_queries, sizeof(BatchQuery) * nq), "pinned queries");
     if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "pinned ctl");
     if (!rc) rc = reset_all(b, b->stream);
     if (!rc) rc = cuda_fail(cudaStreamSynchronize(b->stream), "batch init");
@@ -194,37 +257,16 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
     cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
     int rc = MLMQ_OK;
     if (b->dirty && (rc = reset_all(b, st))) return rc;
-    const size_t l2s = l2_slots(b);
     std::vector<long long> key;
     key.reserve(2 * (size_t)nq);
     b->n_of.assign((size_t)nq, 0);
     for (int q = 0; q < nq; q++) {
         const mlmq_graph *g = graphs[q];
-        PlainParams &p = b->h_params[q];
-        std::memset(&p, 0, sizeof(p));
-        p.n = g->n;
-        p.row = g->d_row;
-        p.arcs = g->d_arcs;
-        p.dist = b->d_dist + (size_t)q * b->max_n;
-        p.src = srcs[q];
-        p.l2 = b->d_l2 + (size_t)q * l2s;
-        p.l3 = b->d_l3 + ((size_t)q << b->l3_log);
-        p.l3bits = b->d_l3bits + (size_t)q * b->bits_words;
-        p.ctlw = b->d_ctl + (size_t)q * CTL_STRIDE;
-        p.nb = b->cfg.bucket_num;
-        p.bm = b->cfg.bucket_max;
-        p.batch = b->cfg.l2_batch;
-        p.min_read = b->cfg.min_read;
-        p.large = b->cfg.large_degree;
-        p.l1_spill = b->cfg.l1_spill;
-        p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
-        p.l1_keep = b->cfg.l1_keep;
-        p.precheck = b->cfg.relax_precheck;
-        p.delta = (unsigned)b->cfg.delta;
-        p.l2_log = b->l2_log;
-        p.l3_log = b->l3_log;
-        p.workers = b->workers;
-        p.timeout_ns = (unsigned long long)b->cfg.timeout_ms * 1000000ull;
+        BatchQuery &qy = b->h_queries[q];
+        qy.row = g->d_row;
+        qy.arcs = g->d_arcs;
+        qy.n = g->n;
+        qy.src = srcs[q];
         b->n_of[q] = g->n;
         key.push_back((long long)(uintptr_t)g);
         key.push_back(srcs[q]);
@@ -332,8 +374,8 @@ extern "C" void mlmq_batch_destroy(mlmq_batch *b) {
     cudaFree(b->d_l3);
     cudaFree(b->d_l3bits);
     cudaFree(b->d_ctl);
-    cudaFree(b->d_params);
-    if (b->h_params) cudaFreeHost(b->h_params);
+    cudaFree(b->d_queries);
+    if (b->h_queries) cudaFreeHost(b->h_queries);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->done) cudaEventDestroy(b->done);
     if (b->stream) cudaStreamDestroy(b->stream);

@@ -5,24 +5,39 @@
 
 namespace mlmq {
 
-__global__ void __launch_bounds__(1024, 1) sssp_plain_kernel(PlainParams p) {
-    plain_body<ArcsInterleaved>(p, blockIdx.x, gridDim.x);
+// K = 32-arc relaxation rounds a warp keeps in flight (mlmq_config.relax_unroll).
+// One round needs few registers, so its variant takes CTAs of up to 1024
+// threads; the unrolled variants get the register budget of 800 threads.
+template <int K>
+__global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
+    sssp_plain_kernel(PlainParams p) {
+    plain_body<ArcsInterleaved, K>(p, blockIdx.x, gridDim.x);
 }
+
+namespace {
+const void *plain_kernel(int unroll) {
+    switch (unroll) {
+        case 1: return (const void *)sssp_plain_kernel<1>;
+        case 2: return (const void *)sssp_plain_kernel<2>;
+        default: return (const void *)sssp_plain_kernel<4>;
+    }
+}
+}  // namespace
 
 // ---- host side ----------------------------------------------------------------
 
 size_t plain_smem_bytes(int workers) { return (size_t)workers * (L1_CAP + 32) * sizeof(uint2); }
 
-cudaError_t plain_max_blocks_per_sm(int workers, int *blocks) {
+cudaError_t plain_max_blocks_per_sm(int workers, int unroll, int *blocks) {
     const int threads = 32 * (workers + 1);
     const size_t smem = plain_smem_bytes(workers);
-    cudaError_t e = cudaFuncSetAttribute(sssp_plain_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const void *k = plain_kernel(unroll);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, sssp_plain_kernel, threads, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k, threads, smem);
 }
 
-cudaError_t plain_launch(const PlainParams &p, int grid, cudaStream_t stream) {
+cudaError_t plain_launch(const PlainParams &p, int unroll, int grid, cudaStream_t stream) {
     const int threads = 32 * (p.workers + 1);
     const size_t smem = plain_smem_bytes(p.workers);
     cudaLaunchConfig_t cfg = {};
@@ -35,7 +50,8 @@ cudaError_t plain_launch(const PlainParams &p, int grid, cudaStream_t stream) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, sssp_plain_kernel, p);
+    void *args[] = {const_cast<PlainParams *>(&p)};
+    return cudaLaunchKernelExC(&cfg, plain_kernel(unroll), args);
 }
 
 }  // namespace mlmq

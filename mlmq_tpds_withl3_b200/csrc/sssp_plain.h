@@ -8,11 +8,17 @@ namespace mlmq {
 
 struct PlainParams;
 
+// Most threads per CTA of the persistent kernels that keep more than one
+// relaxation round in flight (24 worker warps + the manager): their register
+// budget is sized for it.
+constexpr int PLAIN_MAX_THREADS = 800;
+
 // Dynamic shared memory of one CTA with `workers` worker warps.
 size_t plain_smem_bytes(int workers);
-// CTAs of the kernel that fit on one SM (also sets the shared-memory limit).
-cudaError_t plain_max_blocks_per_sm(int workers, int *blocks);
+// CTAs of the kernel with `unroll` relaxation rounds in flight (1, 2 or 4)
+// that fit on one SM (also sets the shared-memory limit).
+cudaError_t plain_max_blocks_per_sm(int workers, int unroll, int *blocks);
 // Cooperative launch of `grid` CTAs on `stream`.
-cudaError_t plain_launch(const PlainParams &p, int grid, cudaStream_t stream);
+cudaError_t plain_launch(const PlainParams &p, int unroll, int grid, cudaStream_t stream);
 
 }  // namespace mlmq

@@ -101,7 +101,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
     }
 }
 
-template <class Arcs>
+template <class Arcs, int K>
 __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirror &mir, uint2 *ring,
                                             uint2 *inb, WarpQ &q) {
     const int lane = threadIdx.x & 31;
@@ -138,13 +138,14 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
             }
             __syncwarp();
         }
-        relax_batch<Arcs>(p, q, ring, valid, v, d);
+        relax_batch<Arcs, K>(p, q, ring, valid, v, d);
     }
 }
 
 // `grank`/`gsize`: this CTA's rank in, and the size of, the group of CTAs
-// that serves the query (the whole grid for a single-source launch).
-template <class Arcs>
+// that serves the query (the whole grid for a single-source launch).  K is
+// the number of 32-arc relaxation rounds a warp keeps in flight.
+template <class Arcs, int K>
 __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank, unsigned gsize) {
     extern __shared__ uint2 smem[];
     __shared__ Mirror mir_storage;
@@ -202,7 +203,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     q.pushed = q.l3_pushed = q.relaxed = q.improved = 0ull;
     q.deadline = deadline;
 
-    worker_loop<Arcs>(p, mir, ring, inb, q);
+    worker_loop<Arcs, K>(p, mir, ring, inb, q);
 
     // ---- epilogue: statistics --------------------------------------------------
     unsigned long long relaxed = q.relaxed, improved = q.improved;

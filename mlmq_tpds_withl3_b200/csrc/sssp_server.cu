@@ -109,7 +109,9 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
+template <int K>
+__global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
+    sssp_server_kernel(ServerParams sp) {
     const unsigned g = gridDim.x;
     const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)sp.slots) / g);
     const unsigned lo = (unsigned)(((unsigned long long)s * g + sp.slots - 1) / (unsigned)sp.slots);
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
         p.l3 = sp.l3 + ((size_t)s << p.l3_log);
         p.l3bits = sp.l3bits + (size_t)s * sp.bits_words;
         p.ctlw = c;
-        plain_body<ArcsInterleaved>(p, grank, gsize);
+        plain_body<ArcsInterleaved, K>(p, grank, gsize);
         // A solve that stopped early leaves records in the rings: the group
         // empties them before the slot is reused.
         __shared__ unsigned solve_status;
@@ -217,6 +219,14 @@ __global__ void __launch_bounds__(1024, 1) sssp_server_kernel(ServerParams sp) {
             __threadfence_system();
         }
         if (!ok) return;
+    }
+}
+
+const void *server_kernel(int unroll) {
+    switch (unroll) {
+        case 1: return (const void *)sssp_server_kernel<1>;
+        case 2: return (const void *)sssp_server_kernel<2>;
+        default: return (const void *)sssp_server_kernel<4>;
     }
 }
 
@@ -294,11 +304,10 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
     int bps = 0;
     const int threads = 32 * (sv->workers + 1);
     const size_t smem = plain_smem_bytes(sv->workers);
-    if (!rc) rc = cuda_fail(cudaFuncSetAttribute(sssp_server_kernel,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const void *kern = server_kernel(cfg.relax_unroll);
+    if (!rc) rc = cuda_fail(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem), "server smem");
-    if (!rc) rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_server_kernel,
-                                                                          threads, smem),
+    if (!rc) rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem),
                             "server occupancy");
     if (!rc) {
         sv->grid = cfg.work_blocks > 0 ? std::min(cfg.work_blocks, bps * sms) : bps * sms;
@@ -371,7 +380,8 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
             attr[0].val.cooperative = 1;
             lc.attrs = attr;
             lc.numAttrs = 1;
-            rc = cuda_fail(cudaLaunchKernelEx(&lc, sssp_server_kernel, sp), "server launch");
+            void *args[] = {&sp};
+            rc = cuda_fail(cudaLaunchKernelExC(&lc, kern, args), "server launch");
         }
         if (!rc) rc = cuda_fail(cudaEventRecord(sv->kdone, sv->kstream), "server event");
         sv->running = !rc;

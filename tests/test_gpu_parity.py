@@ -73,6 +73,10 @@ def test_c1_grid512_bit_exact():
     {"l1_keep": 8},
     {"l1_keep": 32, "queue_type": MLMQ_L1V_L2DQ},
     {"relax_precheck": 0},
+    {"relax_unroll": 1},
+    {"relax_unroll": 2, "large_degree": 4},
+    {"relax_unroll": 4, "relax_precheck": 0, "warps_per_block": 24},
+    {"relax_unroll": 1, "warps_per_block": 31},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
