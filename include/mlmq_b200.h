@@ -86,8 +86,10 @@ typedef struct mlmq_config {
     int timeout_ms;      /* device wait limit per solve (default 20000) */
     int l1_keep;         /* on a spill, records kept at the L1 front (0 = spill
                             all, the reference's rule; at most l1_spill) */
-    int relax_precheck;  /* 1: read dist[dst] before atomicMin (default);
-                            0: atomicMin directly (one less dependent load) */
+    int relax_precheck;  /* 1 (default): read dist[dst] first; a smaller
+                            candidate is pushed and written with a
+                            fire-and-forget min (red.min); 0: atomicMin
+                            directly, its returned value decides the push */
     int relax_unroll;    /* rounds of 32 arcs a warp keeps in flight: 1, 2 or
                             4 (default 4; above 1 at most
                             MLMQ_MAX_UNROLLED_WARPS worker warps per CTA) */

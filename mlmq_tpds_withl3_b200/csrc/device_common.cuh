@@ -66,6 +66,10 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
 __device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// atomicMin without a returned value: the issuing warp does not wait for it.
+__device__ __forceinline__ void red_min(int *p, int v) {
+    asm volatile("red.relaxed.gpu.global.min.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

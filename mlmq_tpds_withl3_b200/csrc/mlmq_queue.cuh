@@ -365,7 +365,7 @@ __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile 
         st_relaxed64(l3_slot(p, s), SENT);
         atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
         __threadfence();
-        const unsigned cur = (unsigned)__ldcg(p.dist + v);
+        const unsigned cur = min((unsigned)__ldcg(p.dist + v), rec_d(r));
         inb[lane] = make_uint2(v, cur);
         dmin = cur;
     }
@@ -422,6 +422,10 @@ __device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uin
         cur[k] = INT_MAX;
         if (ok[k] && (p.precheck || nd[k] >= (unsigned)INT_MAX)) cur[k] = __ldcg(p.dist + dst[k]);
     }
+    // With the pre-check the distance update is a fire-and-forget red.min and
+    // the record is pushed when it beat the distance read: a push that a
+    // concurrent smaller update made redundant is a stale record, which the
+    // reader drops.  Without it, atomicMin's returned value decides.
     bool win[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -430,7 +434,12 @@ __device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uin
             if (nd[k] >= (unsigned)INT_MAX) {
                 if (cur[k] == INT_MAX) q.range_hit = 1;  // a finite distance would not fit
             } else if ((int)nd[k] < cur[k]) {
-                win[k] = (int)nd[k] < atomicMin(p.dist + dst[k], (int)nd[k]);
+                if (p.precheck) {
+                    red_min(p.dist + dst[k], (int)nd[k]);
+                    win[k] = true;
+                } else {
+                    win[k] = (int)nd[k] < atomicMin(p.dist + dst[k], (int)nd[k]);
+                }
             }
         }
     }
@@ -456,8 +465,11 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         const int cur = __ldcg(p.dist + v);
         const int rb = __ldg(p.row + v);
         const int re = __ldg(p.row + v + 1);
+        // Relax with the record's own distance: it is the length of a real
+        // path, and with the fire-and-forget distance updates below the
+        // update that made the record may not be visible here yet.
         if ((int)d <= cur) {
-            du = (unsigned)cur;
+            du = d;
             beg = rb;
             deg = re - rb;
         }
