@@ -93,6 +93,9 @@ typedef struct mlmq_config {
     int relax_unroll;    /* rounds of 32 arcs a warp keeps in flight: 1, 2 or
                             4 (default 4; above 1 at most
                             MLMQ_MAX_UNROLLED_WARPS worker warps per CTA) */
+    int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
+                            32-byte tile (up to 4 arcs inline, else its CSR
+                            range); 0: row offsets, then arcs */
 } mlmq_config;
 
 /* Fills *cfg with the reference's defaults (common.h:24-34, sssp.cuh:20,

@@ -76,7 +76,7 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
          extra=None):
     """Returns (config, report).  Candidates: delta from delta_candidates(),
     then warps per CTA in {8, 16, 24} at the best delta, then 1, 2 or 4
-    relaxation rounds in flight."""
+    relaxation rounds in flight, then vertex tiles on or off."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -104,9 +104,10 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         t = measure(over)
         if t < best_t:
             best, best_t = over, t
-    # Relaxation rounds in flight per warp (default 4) at the best shape.
-    for unroll in (1, 2):
-        over = {**best, "relax_unroll": unroll}
+    # Relaxation rounds in flight per warp (default 4), then the adjacency
+    # layout (vertex tiles, default on) at the best shape.
+    for extra_opt in ({"relax_unroll": 1}, {"relax_unroll": 2}, {"vertex_tiles": 0}):
+        over = {**best, **extra_opt}
         t = measure(over)
         if t < best_t:
             best, best_t = over, t

@@ -12,6 +12,13 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int NB_MAX = 32;      // L2 buckets; lane b of a warp owns bucket b's claim
 constexpr int L1_CAP = 64;      // SLF ring slots per warp (reference MAX_L1SLF_BATCH_SIZE)
 constexpr unsigned long long SENT = ~0ull;  // empty ring slot
+// Vertex tiles: 32 bytes per vertex, {dst, weight} x TILE_ARCS inline (unused
+// slots dst = -1), or {TILE_CSR, first arc, degree, ...} for higher degree.
+constexpr int TILE_ARCS = 4;
+constexpr int TILE_CSR = -2;
+// 8-byte shared-memory slots per worker warp: L1 ring, L2/L3 read buffer,
+// staged tile arcs.
+constexpr int WARP_SMEM_SLOTS = L1_CAP + 32 + 32 * TILE_ARCS;
 
 // ---- control block: 32-bit words, one 128-byte line per group ------------
 namespace ctl {

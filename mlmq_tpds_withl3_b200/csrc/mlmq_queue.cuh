@@ -57,6 +57,7 @@ struct PlainParams {
     int n;
     const int *__restrict__ row;
     const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
+    const int4 *__restrict__ tiles; // 2 per vertex, or null: read row offsets instead
     const int *__restrict__ col;    // caller's CSR arrays, read in place (ArcsSplit)
     const int *__restrict__ w;
     int *dist;
@@ -395,28 +396,17 @@ struct ArcsSplit {
     }
 };
 
-// Relaxes up to K rounds of 32 arcs (lane-distributed: round k gives this lane
-// arc ai[k] of a vertex at distance du[k] when ok[k]) and feeds the winners to
-// L1.  The rounds' arc loads, then their destination-distance loads, then
-// their atomicMins are issued back to back, so a warp keeps K independent
-// dependent-load chains in flight instead of one; `rounds` (warp-uniform) is
-// the number of rounds that hold any arc.
-template <class Arcs, int K>
-__device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uint2 *ring,
-                                             const bool (&ok)[K], const int (&ai)[K],
-                                             const unsigned (&du)[K], int rounds) {
-    unsigned dst[K], nd[K];
+// Relaxes up to K rounds of 32 arcs whose destinations and candidate
+// distances are known (round k: this lane's arc to dst[k] with candidate
+// nd[k] when ok[k]) and feeds the winners to L1.  The rounds' destination-
+// distance loads, then their updates, are issued back to back, so a warp
+// keeps K independent chains in flight; `rounds` (warp-uniform) bounds the
+// rounds that hold any arc.
+template <int K>
+__device__ __forceinline__ void relax_known(const PlainParams &p, WarpQ &q, uint2 *ring,
+                                            const bool (&ok)[K], const unsigned (&dst)[K],
+                                            const unsigned (&nd)[K], int rounds) {
     int cur[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        dst[k] = 0u;
-        nd[k] = 0u;
-        if (ok[k]) {
-            const int2 a = Arcs::load(p, ai[k]);
-            dst[k] = (unsigned)a.x;
-            nd[k] = du[k] + (unsigned)a.y;
-        }
-    }
 #pragma unroll
     for (int k = 0; k < K; k++) {
         cur[k] = INT_MAX;
@@ -452,24 +442,73 @@ __device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uin
     }
 }
 
-// Relaxes up to 32 records (one per lane) and feeds the winners to L1.
+// Loads the arcs of K lane-distributed rounds (round k: this lane's arc ai[k]
+// of a vertex at distance du[k] when ok[k]; a negative ai[k] is
+// INT_MIN + an index into this warp's staged tile arcs), then relaxes them.
 template <class Arcs, int K>
-__device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
-                                            unsigned v, unsigned d) {
+__device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uint2 *ring,
+                                             const int2 *stage, const bool (&ok)[K], const int (&ai)[K],
+                                             const unsigned (&du)[K], int rounds) {
+    unsigned dst[K], nd[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        dst[k] = 0u;
+        nd[k] = 0u;
+        if (ok[k]) {
+            const int2 a = ai[k] < 0 ? stage[(unsigned)ai[k] - 0x80000000u] : Arcs::load(p, ai[k]);
+            dst[k] = (unsigned)a.x;
+            nd[k] = du[k] + (unsigned)a.y;
+        }
+    }
+    relax_known<K>(p, q, ring, ok, dst, nd, rounds);
+}
+
+// Relaxes up to 32 records (one per lane) and feeds the winners to L1.
+// `stage` is this warp's TILE_ARCS * 32 arcs of shared memory.
+template <class Arcs, int K>
+__device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring,
+                                            int2 *stage, bool valid, unsigned v, unsigned d) {
     const int lane = threadIdx.x & 31;
     int beg = 0, deg = 0;
-    unsigned du = 0;
-    if (valid) {
+    // Records are relaxed with their own distance: it is the length of a real
+    // path, and with the fire-and-forget distance updates the update that
+    // made the record may not be visible here yet.
+    const unsigned du = d;
+    if (p.tiles) {
+        // Vertex tile: the distance (stale check) and the 32-byte tile are
+        // independent loads.  A vertex of degree <= TILE_ARCS has all its arcs
+        // in the tile: they are staged in shared memory and its `beg` becomes
+        // INT_MIN + its stage offset, so the arc distribution below handles
+        // staged and CSR arcs alike and keeps the CSR path's arc order.
+        int cur = INT_MAX;
+        int4 ta = make_int4(-1, 0, -1, 0), tb = ta;
+        if (valid) {
+            cur = __ldcg(p.dist + v);
+            ta = __ldg(p.tiles + 2 * (size_t)v);
+            tb = __ldg(p.tiles + 2 * (size_t)v + 1);
+        }
+        if (valid && (int)d <= cur) {
+            if (ta.x == TILE_CSR) {
+                beg = ta.y;
+                deg = ta.z;
+            } else {
+                int2 *st = stage + TILE_ARCS * lane;
+                st[0] = make_int2(ta.x, ta.y);
+                st[1] = make_int2(ta.z, ta.w);
+                st[2] = make_int2(tb.x, tb.y);
+                st[3] = make_int2(tb.z, tb.w);
+                deg = (ta.x >= 0) + (ta.z >= 0) + (tb.x >= 0) + (tb.z >= 0);
+                beg = INT_MIN + TILE_ARCS * lane;
+            }
+        }
+        __syncwarp();
+    } else if (valid) {
         // The three loads are independent: issue them together rather than
         // after the stale check.
         const int cur = __ldcg(p.dist + v);
         const int rb = __ldg(p.row + v);
         const int re = __ldg(p.row + v + 1);
-        // Relax with the record's own distance: it is the length of a real
-        // path, and with the fire-and-forget distance updates below the
-        // update that made the record may not be visible here yet.
         if ((int)d <= cur) {
-            du = d;
             beg = rb;
             deg = re - rb;
         }
@@ -494,7 +533,7 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
                 ai[k] = lb + e;
                 uu[k] = lu;
             }
-            relax_rounds<Arcs, K>(p, q, ring, ok, ai, uu, (ld - e0 + 31) >> 5);
+            relax_rounds<Arcs, K>(p, q, ring, stage, ok, ai, uu, (ld - e0 + 31) >> 5);
         }
     }
     if (deg >= p.large) deg = 0;
@@ -528,7 +567,7 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
             ok[k] = e < total;
             ai[k] = ob + (e - oo);
         }
-        relax_rounds<Arcs, K>(p, q, ring, ok, ai, uu, (total - e0 + 31) >> 5);
+        relax_rounds<Arcs, K>(p, q, ring, stage, ok, ai, uu, (total - e0 + 31) >> 5);
     }
 }
 

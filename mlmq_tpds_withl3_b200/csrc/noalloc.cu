@@ -144,6 +144,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.n = n;
     p.row = d_row;
     p.arcs = nullptr;
+    p.tiles = nullptr;  // the caller's CSR is read in place
     p.col = d_col;
     p.w = d_w;
     p.dist = d_dist;

@@ -37,6 +37,30 @@ __global__ void interleave_kernel(const int *__restrict__ col, const int *__rest
         arcs[i] = make_int2(col[i], w[i]);
 }
 
+// One 32-byte tile per vertex (layout in mlmq_queue.cuh): up to TILE_ARCS
+// arcs inline, unused slots with dst -1; a vertex of higher degree holds
+// {TILE_CSR, first arc, degree} instead.
+__global__ void tile_kernel(const int *__restrict__ row, const int2 *__restrict__ arcs,
+                            int4 *tiles, int n) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int beg = row[v], deg = row[v + 1] - beg;
+        int t[8] = {-1, 0, -1, 0, -1, 0, -1, 0};
+        if (deg > TILE_ARCS) {
+            t[0] = TILE_CSR;
+            t[1] = beg;
+            t[2] = deg;
+        } else {
+            for (int i = 0; i < deg; i++) {
+                const int2 a = arcs[beg + i];
+                t[2 * i] = a.x;
+                t[2 * i + 1] = a.y;
+            }
+        }
+        tiles[2 * (size_t)v] = make_int4(t[0], t[1], t[2], t[3]);
+        tiles[2 * (size_t)v + 1] = make_int4(t[4], t[5], t[6], t[7]);
+    }
+}
+
 __global__ void fill_kernel(int *p, int64_t n, int v) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -99,6 +123,7 @@ int validate_config(const mlmq_config &c) {
     if (c.relax_precheck != 0 && c.relax_precheck != 1) return MLMQ_ERR_ARG;
     if (c.relax_unroll != 1 && c.relax_unroll != 2 && c.relax_unroll != 4) return MLMQ_ERR_ARG;
     if (c.relax_unroll > 1 && c.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
+    if (c.vertex_tiles != 0 && c.vertex_tiles != 1) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -168,6 +193,7 @@ extern "C" int mlmq_config_default(mlmq_config *cfg) {
     cfg->l1_keep = 0;
     cfg->relax_precheck = 1;
     cfg->relax_unroll = 4;
+    cfg->vertex_tiles = 1;
     int rc = MLMQ_OK;
     bool have = false;
     int d = env_int("BENCH_DELTA", 200000, &have);
@@ -209,6 +235,13 @@ extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const 
         interleave_kernel<<<blocks, 256>>>(d_col, d_w, g->d_arcs, m);
         rc = cuda_fail(cudaGetLastError(), "interleave launch");
         if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "interleave");
+    }
+    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_tiles, 2 * sizeof(int4) * (size_t)n), "cudaMalloc(tiles)");
+    if (!rc) {
+        int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 16);
+        tile_kernel<<<blocks, 256>>>(d_row, g->d_arcs, g->d_tiles, n);
+        rc = cuda_fail(cudaGetLastError(), "tile launch");
+        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "tiles");
     }
     if (rc) {
         mlmq_graph_free(g);
@@ -258,6 +291,7 @@ extern "C" int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m) {
 extern "C" void mlmq_graph_free(mlmq_graph *g) {
     if (!g) return;
     if (g->d_arcs) cudaFree(g->d_arcs);
+    if (g->d_tiles) cudaFree(g->d_tiles);
     if (g->own_row && g->d_row) cudaFree(g->d_row);
     delete g;
 }
@@ -340,6 +374,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.n = s->g->n;
     p.row = s->g->d_row;
     p.arcs = s->g->d_arcs;
+    p.tiles = s->cfg.vertex_tiles ? s->g->d_tiles : nullptr;
     p.col = nullptr;
     p.w = nullptr;
     p.dist = s->d_dist;

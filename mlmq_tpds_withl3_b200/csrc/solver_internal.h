@@ -14,6 +14,7 @@ struct mlmq_graph {
     int *d_row = nullptr;   // n + 1 row offsets (owned when own_row)
     bool own_row = false;
     int2 *d_arcs = nullptr; // m interleaved {dst, weight} (always owned)
+    int4 *d_tiles = nullptr; // 2 per vertex: the vertex tile (mlmq_queue.cuh; always owned)
 };
 
 struct mlmq_solver {

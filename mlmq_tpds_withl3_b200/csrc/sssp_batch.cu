@@ -36,6 +36,7 @@ constexpr int CTL_STRIDE = 512;  // words per slot control block (2 KiB, padded)
 struct BatchQuery {
     const int *row;
     const int2 *arcs;
+    const int4 *tiles;
     int n, src;
 };
 struct BatchParams {
@@ -45,9 +46,10 @@ struct BatchParams {
     int nq;
 };
 
+// Batched slots use few warps per CTA, so every variant gets the register
+// budget of PLAIN_MAX_THREADS threads.
 template <int K>
-__global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
-    sssp_batch_kernel(BatchParams bp) {
+__global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_batch_kernel(BatchParams bp) {
     const unsigned g = gridDim.x;
     const unsigned nq = (unsigned)bp.nq;
     const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * nq) / g);
@@ -58,6 +60,7 @@ __global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
     const BatchQuery qy = bp.queries[s];
     p.row = qy.row;
     p.arcs = qy.arcs;
+    p.tiles = qy.tiles;
     p.n = qy.n;
     p.src = qy.src;
     p.dist = bp.base.dist + s * bp.dist_stride;
@@ -185,6 +188,7 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
         cfg.warps_per_block = 8;
     }
     if ((rc = validate_config(cfg))) return rc;
+    if (cfg.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
     int sms = 0;
     if ((rc = device_sm_count(&sms))) return rc;
     auto *b = new (std::nothrow) mlmq_batch;
@@ -203,7 +207,7 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
         const size_t smem = plain_smem_bytes(b->workers);
         const void *k = batch_kernel(cfg.relax_unroll);
         rc = cuda_fail(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem), "batch smem");
+                                            (int)plain_smem_limit()), "batch smem");
         if (!rc)
             rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem),
                            "batch occupancy");
@@ -265,6 +269,7 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         BatchQuery &qy = b->h_queries[q];
         qy.row = g->d_row;
         qy.arcs = g->d_arcs;
+        qy.tiles = b->cfg.vertex_tiles ? g->d_tiles : nullptr;
         qy.n = g->n;
         qy.src = srcs[q];
         b->n_of[q] = g->n;

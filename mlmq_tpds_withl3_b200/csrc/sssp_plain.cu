@@ -26,13 +26,15 @@ const void *plain_kernel(int unroll) {
 
 // ---- host side ----------------------------------------------------------------
 
-size_t plain_smem_bytes(int workers) { return (size_t)workers * (L1_CAP + 32) * sizeof(uint2); }
+size_t plain_smem_bytes(int workers) { return (size_t)workers * WARP_SMEM_SLOTS * sizeof(uint2); }
+size_t plain_smem_limit() { return plain_smem_bytes(31); }
 
 cudaError_t plain_max_blocks_per_sm(int workers, int unroll, int *blocks) {
     const int threads = 32 * (workers + 1);
     const size_t smem = plain_smem_bytes(workers);
     const void *k = plain_kernel(unroll);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)plain_smem_limit());
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k, threads, smem);
 }

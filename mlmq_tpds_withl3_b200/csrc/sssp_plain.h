@@ -15,6 +15,11 @@ constexpr int PLAIN_MAX_THREADS = 800;
 
 // Dynamic shared memory of one CTA with `workers` worker warps.
 size_t plain_smem_bytes(int workers);
+// Dynamic shared-memory limit set on every persistent kernel: the largest
+// CTA any configuration may launch (31 worker warps).  One limit for all
+// solvers, so creating a solver with a smaller CTA never lowers the limit
+// below what another live solver launches with.
+size_t plain_smem_limit();
 // CTAs of the kernel with `unroll` relaxation rounds in flight (1, 2 or 4)
 // that fit on one SM (also sets the shared-memory limit).
 cudaError_t plain_max_blocks_per_sm(int workers, int unroll, int *blocks);

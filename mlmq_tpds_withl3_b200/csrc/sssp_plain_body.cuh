@@ -103,7 +103,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
 
 template <class Arcs, int K>
 __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirror &mir, uint2 *ring,
-                                            uint2 *inb, WarpQ &q) {
+                                            uint2 *inb, int2 *stage, WarpQ &q) {
     const int lane = threadIdx.x & 31;
     for (;;) {
         if (mir.exit) break;
@@ -138,7 +138,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
             }
             __syncwarp();
         }
-        relax_batch<Arcs, K>(p, q, ring, valid, v, d);
+        relax_batch<Arcs, K>(p, q, ring, stage, valid, v, d);
     }
 }
 
@@ -191,8 +191,9 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         return;
     }
 
-    uint2 *ring = smem + (size_t)warp * (L1_CAP + 32);
+    uint2 *ring = smem + (size_t)warp * WARP_SMEM_SLOTS;
     uint2 *inb = ring + L1_CAP;
+    int2 *stage = reinterpret_cast<int2 *>(inb + 32);
     WarpQ q;
     q.l1_head = q.l1_tail = q.l1_size = 0;
     q.c_lo = q.c_hi = 0u;
@@ -203,7 +204,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     q.pushed = q.l3_pushed = q.relaxed = q.improved = 0ull;
     q.deadline = deadline;
 
-    worker_loop<Arcs, K>(p, mir, ring, inb, q);
+    worker_loop<Arcs, K>(p, mir, ring, inb, stage, q);
 
     // ---- epilogue: statistics --------------------------------------------------
     unsigned long long relaxed = q.relaxed, improved = q.improved;

@@ -38,7 +38,7 @@ namespace {
 constexpr int SRV_CTL_STRIDE = 512;  // words per slot control block
 // Words of the slot control block used by the server around a solve (the
 // solve itself uses words below ctl::WORDS).
-constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs (2 words each), n, src
+constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs, tiles (2 words each), n, src
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_BAR_COUNT = 488;
@@ -56,6 +56,7 @@ struct alignas(64) SlotCommand {
     volatile unsigned long long seq;
     const int *row;
     const int2 *arcs;
+    const int4 *tiles;
     int n;
     int src;
 };
@@ -109,9 +110,10 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
     return ok != 0;
 }
 
+// Server slots use few warps per CTA, so every variant gets the register
+// budget of PLAIN_MAX_THREADS threads.
 template <int K>
-__global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
-    sssp_server_kernel(ServerParams sp) {
+__global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(ServerParams sp) {
     const unsigned g = gridDim.x;
     const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)sp.slots) / g);
     const unsigned lo = (unsigned)(((unsigned long long)s * g + sp.slots - 1) / (unsigned)sp.slots);
@@ -147,6 +149,9 @@ __global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
                         c[SRV_CMD + 3] = (unsigned)(arcs >> 32);
                         c[SRV_CMD + 4] = (unsigned)sp.cmd[s].n;
                         c[SRV_CMD + 5] = (unsigned)sp.cmd[s].src;
+                        const unsigned long long tiles = (unsigned long long)sp.cmd[s].tiles;
+                        c[SRV_CMD + 6] = (unsigned)tiles;
+                        c[SRV_CMD + 7] = (unsigned)(tiles >> 32);
                         __threadfence();
                         // publish the sequence number (low 32 bits) to the group
                         st_release(c + SRV_GO, (unsigned)q);
@@ -179,6 +184,7 @@ __global__ void __launch_bounds__(K == 1 ? 1024 : PLAIN_MAX_THREADS, 1)
         const volatile unsigned *cmd = c + SRV_CMD;
         p.row = (const int *)(((unsigned long long)cmd[1] << 32) | cmd[0]);
         p.arcs = (const int2 *)(((unsigned long long)cmd[3] << 32) | cmd[2]);
+        p.tiles = (const int4 *)(((unsigned long long)cmd[7] << 32) | cmd[6]);
         p.n = (int)cmd[4];
         p.src = (int)cmd[5];
         p.dist = sp.dist + (size_t)s * sp.max_n;
@@ -278,6 +284,7 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         cfg.warps_per_block = 8;
     }
     if ((rc = validate_config(cfg))) return rc;
+    if (cfg.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
     int sms = 0;
     if ((rc = device_sm_count(&sms))) return rc;
     auto *sv = new (std::nothrow) mlmq_server;
@@ -306,7 +313,7 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
     const size_t smem = plain_smem_bytes(sv->workers);
     const void *kern = server_kernel(cfg.relax_unroll);
     if (!rc) rc = cuda_fail(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem), "server smem");
+                                                 (int)plain_smem_limit()), "server smem");
     if (!rc) rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem),
                             "server occupancy");
     if (!rc) {
@@ -420,6 +427,7 @@ extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src,
     SlotCommand &cmd = sv->h_cmd[free_slot];
     cmd.row = g->d_row;
     cmd.arcs = g->d_arcs;
+    cmd.tiles = sv->cfg.vertex_tiles ? g->d_tiles : nullptr;
     cmd.n = g->n;
     cmd.src = src;
     std::atomic_thread_fence(std::memory_order_release);

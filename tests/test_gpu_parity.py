@@ -77,6 +77,8 @@ def test_c1_grid512_bit_exact():
     {"relax_unroll": 2, "large_degree": 4},
     {"relax_unroll": 4, "relax_precheck": 0, "warps_per_block": 24},
     {"relax_unroll": 1, "warps_per_block": 31},
+    {"vertex_tiles": 0},
+    {"vertex_tiles": 0, "relax_precheck": 0, "relax_unroll": 1},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
@@ -85,6 +87,18 @@ def test_queue_configurations(cfg):
     ref, _ = oracle_lib.sssp_i32(g, 5)
     s = Solver(DeviceGraph.upload(g), cfg)
     assert np.array_equal(s.solve(5).dist(), ref)
+
+
+def test_live_solvers_with_different_cta_sizes():
+    """A solver created after another one with a larger CTA must not break
+    the first one's launches (the kernel's shared-memory limit is shared)."""
+    g = HostGraph.grid(96, 96, seed=6)
+    dg = DeviceGraph.upload(g)
+    big = Solver(dg, {"warps_per_block": 24})
+    small = Solver(dg, {"warps_per_block": 4})
+    ref, _ = oracle_lib.sssp_i32(g, 7)
+    for s in (big, small, big):
+        assert np.array_equal(s.solve(7).dist(), ref)
 
 
 def test_knn_and_rmat_medium():
