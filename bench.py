@@ -381,10 +381,15 @@ def run_batched(args):
 
     g, srcs = load_workload("c4", args.sources)
     dg = DeviceGraph.upload(g)
-    bcfg = default_config(delta=200000, warps_per_block=8)
+    queries = [(dg, s) for s in srcs]
+    tune_report = None
+    if args.no_tune:
+        bcfg = default_config(delta=200000, warps_per_block=8)
+    else:
+        from mlmq_tpds_withl3_b200 import autotune
+        bcfg, tune_report = autotune.tune_batch(queries, g.n)
     batch = BatchSolver(len(srcs), g.n, bcfg)
     stream = torch.cuda.Stream()
-    queries = [(dg, s) for s in srcs]
 
     # Correctness: oracle on a few sources, the plain solver on every source.
     check_q = list(range(0, len(srcs), max(1, len(srcs) // 4)))[:4]
@@ -392,7 +397,13 @@ def run_batched(args):
     batch.run(queries, use_graph=True)
     correct = all(np.array_equal(batch.dist(q), ref[i]) for i, q in enumerate(check_q))
     del ref
-    plain = Solver(dg, default_config(delta=200000))
+    # The back-to-back baseline gets its own tuned single-solve configuration.
+    if args.no_tune:
+        pcfg = default_config(delta=200000)
+    else:
+        from mlmq_tpds_withl3_b200 import autotune
+        pcfg, _ = autotune.tune(dg, g, srcs[:2], kind="c4-plain", use_cache=False)
+    plain = Solver(dg, pcfg)
     plain_ms, works, reached = [], [], []
     for q, s in enumerate(srcs):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -439,11 +450,17 @@ def run_batched(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator)",
         "config": {"workload": WORKLOAD_TEXT["c4"], "n": g.n, "m": g.m, "sources": len(srcs),
-                   "delta": 200000, "warps_per_block": 8, "grid": batch.grid,
+                   "delta": bcfg.delta, "warps_per_block": bcfg.warps_per_block,
+                   "l1_ahead": bcfg.l1_ahead, "relax_unroll": bcfg.relax_unroll,
+                   "grid": batch.grid,
                    "cuda_graph": True, "l2": "inputs (6.1 GB distances, 0.7 GB arcs) exceed L2"},
         "correct": bool(correct),
         "gteps": work_step * args.steps / total_s / 1e9,
         "plain_back_to_back": {"qps": plain_qps, "ms_per_query_p50": float(np.median(plain_ms)),
+                               "config": {"delta": pcfg.delta, "warps_per_block": pcfg.warps_per_block,
+                                          "relax_unroll": pcfg.relax_unroll,
+                                          "l1_ahead": pcfg.l1_ahead,
+                                          "vertex_tiles": pcfg.vertex_tiles},
                                "gteps": work_step / (np.sum(plain_ms) / 1e3) / 1e9},
         "speedup_vs_plain_qps": qps / plain_qps,
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
@@ -456,6 +473,8 @@ def run_batched(args):
                      "algorithmic_bytes_per_launch": bytes_step},
         "clocks": sampler.summary(), "gpu_launches": len(events),
     }
+    if tune_report:
+        line["autotune"] = {"config": tune_report["config"], "trials": len(tune_report["trials"])}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

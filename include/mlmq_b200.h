@@ -93,6 +93,10 @@ typedef struct mlmq_config {
     int relax_unroll;    /* rounds of 32 arcs a warp keeps in flight: 1, 2 or
                             4 (default 4; above 1 at most
                             MLMQ_MAX_UNROLLED_WARPS worker warps per CTA) */
+    int l1_ahead;        /* a winner stays in the warp's L1 only while its
+                            bucket is below first + l1_ahead, else it goes
+                            to L2/L3 through the warp's outbox (default 4;
+                            0: no limit, the reference's L1) */
     int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
                             32-byte tile (up to 4 arcs inline, else its CSR
                             range); 0: row offsets, then arcs */
@@ -252,6 +256,12 @@ int mlmq_batch_query_status(const mlmq_batch *b, int q, unsigned *status,
                             mlmq_solve_stats *st);
 int mlmq_batch_dist(mlmq_batch *b, int q, int **d_dist);
 int mlmq_batch_copy_dist(mlmq_batch *b, int q, int *h_dist);
+/* Copies the first `count` 32-bit words of query q's queue control block as
+ * they were when its last launch ended (queue counters, `first`, status; the
+ * layout is device_common.cuh's ctl namespace): a snapshot for diagnosing a
+ * solve that timed out, the role of the reference's hang-diagnostic counters
+ * (SSSP/sssp_run.cu HANG_DIAG, L3_LIVE_SNAPSHOT). */
+int mlmq_batch_control(const mlmq_batch *b, int q, unsigned *words, int count);
 void mlmq_batch_destroy(mlmq_batch *b);
 
 /* ---- 2d. continuous-batching server ---------------------------------------

@@ -61,7 +61,7 @@ class Config(ctypes.Structure):
         "queue_type", "delta", "work_blocks", "warps_per_block", "l2_batch",
         "bucket_num", "bucket_max", "min_read", "large_degree", "l1_spill",
         "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck",
-        "relax_unroll", "vertex_tiles")]
+        "relax_unroll", "l1_ahead", "vertex_tiles")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -131,6 +131,7 @@ _sig("mlmq_batch_wait", c_int, c_vp)
 _sig("mlmq_batch_query_status", c_int, c_vp, c_int, ctypes.POINTER(c_u32),
      ctypes.POINTER(SolveStats))
 _sig("mlmq_batch_dist", c_int, c_vp, c_int, ctypes.POINTER(c_vp))
+_sig("mlmq_batch_control", c_int, c_vp, c_int, ctypes.POINTER(c_u32), c_int)
 _sig("mlmq_batch_copy_dist", c_int, c_vp, c_int, c_vp)
 _sig("mlmq_batch_destroy", None, c_vp)
 # continuous-batching server

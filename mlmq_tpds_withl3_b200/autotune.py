@@ -76,7 +76,8 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
          extra=None):
     """Returns (config, report).  Candidates: delta from delta_candidates(),
     then warps per CTA in {8, 16, 24} at the best delta, then 1, 2 or 4
-    relaxation rounds in flight, then vertex tiles on or off."""
+    relaxation rounds in flight, then vertex tiles on or off, then the L1
+    run-ahead bound."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -106,7 +107,8 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
             best, best_t = over, t
     # Relaxation rounds in flight per warp (default 4), then the adjacency
     # layout (vertex tiles, default on) at the best shape.
-    for extra_opt in ({"relax_unroll": 1}, {"relax_unroll": 2}, {"vertex_tiles": 0}):
+    for extra_opt in ({"relax_unroll": 1}, {"relax_unroll": 2}, {"vertex_tiles": 0},
+                      {"l1_ahead": 0}, {"l1_ahead": 16}):
         over = {**best, **extra_opt}
         t = measure(over)
         if t < best_t:
@@ -115,6 +117,36 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
     if use_cache:
         store_cache(key, {"config": best, "seconds": best_t})
     return default_config(**{**best, **base}), report
+
+
+def tune_batch(queries, max_vertices, candidates=None, base=None):
+    """Times one batched launch of `queries` ([(DeviceGraph, source)]) per
+    candidate configuration (bucket width, L1 run-ahead bound, relaxation
+    rounds) and returns (config, report) for the fastest.  A batch is bound
+    by the GPU's total relaxation throughput rather than by one query's
+    chain of dependent hops, so its best setting differs from a single
+    solve's.  Every candidate gives the same exact distances."""
+    from .batch import BatchSolver
+    base = dict(base or {"warps_per_block": 8})
+    if candidates is None:
+        candidates = [{"delta": d, "relax_unroll": u}
+                      for d in (50000, 100000, 200000) for u in (2, 4)]
+        candidates += [{"delta": 100000, "relax_unroll": 2, "l1_ahead": a} for a in (0, 2)]
+    results = []
+    for over in candidates:
+        b = BatchSolver(len(queries), max_vertices, {**base, **over})
+        try:
+            b.run(queries)  # warm-up
+            t0 = time.perf_counter()
+            b.run(queries)
+            t = time.perf_counter() - t0
+        finally:
+            b.close()
+        results.append({"config": over, "seconds": t})
+    best = min(results, key=lambda r: r["seconds"])
+    return default_config(**{**base, **best["config"]}), {"config": best["config"],
+                                                          "seconds": best["seconds"],
+                                                          "trials": results}
 
 
 def median_ms(times):

@@ -69,6 +69,12 @@ class BatchSolver:
         check(lib.mlmq_batch_dist(self._h, q, ctypes.byref(p)))
         return p.value
 
+    def control(self, q, count=272):
+        """Query q's control-block words when its last launch ended."""
+        arr = (ctypes.c_uint32 * count)()
+        check(lib.mlmq_batch_control(self._h, q, arr, count), "mlmq_batch_control")
+        return np.frombuffer(arr, dtype=np.uint32).copy()
+
     def stats(self, q):
         st = _lib.SolveStats()
         status = ctypes.c_uint32()

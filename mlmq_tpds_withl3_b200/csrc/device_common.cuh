@@ -17,8 +17,10 @@ constexpr unsigned long long SENT = ~0ull;  // empty ring slot
 constexpr int TILE_ARCS = 4;
 constexpr int TILE_CSR = -2;
 // 8-byte shared-memory slots per worker warp: L1 ring, L2/L3 read buffer,
-// staged tile arcs.
-constexpr int WARP_SMEM_SLOTS = L1_CAP + 32 + 32 * TILE_ARCS;
+// staged tile arcs, outbox of records bound for L2/L3.
+constexpr int OUTBOX_CAP = 64;
+constexpr int OUTBOX_OFF = L1_CAP + 32 + 32 * TILE_ARCS;
+constexpr int WARP_SMEM_SLOTS = OUTBOX_OFF + OUTBOX_CAP;
 
 // ---- control block: 32-bit words, one 128-byte line per group ------------
 namespace ctl {
@@ -27,6 +29,8 @@ constexpr int EXIT = 1;       // 1 = all warps leave the persistent loop
 constexpr int STATUS = 2;     // ST_* bits
 constexpr int PRESSURE = 3;   // bit b: L2 bucket b is filling, new pushes go to L3
 constexpr int U_PRESSURE = 4; // 1: the urgent ring is filling, its pushes go to L3
+constexpr int L3_MIN = 5;     // smallest distance pushed to L3 since the last L3 epoch
+constexpr int L3_EPOCH = 6;   // L3 slots below this may be read (set when an epoch opens)
 constexpr int BAR_COUNT = 8;  // grid barrier arrivals (self-resetting)
 constexpr int BAR_GEN = 9;    // grid barrier generation
 constexpr int CREDIT = 32;    // records read from L2/L3 whose work is finished

@@ -68,6 +68,7 @@ struct PlainParams {
     unsigned *ctlw;
     int nb, bm, batch, min_read, large, l1_spill, l1_vector;
     int l1_keep;   // records kept at the L1 front when it spills (0: spill all)
+    int l1_ahead;  // buckets past `first` a winner may be to stay in L1 (0: no limit)
     int precheck;  // read dist[dst] before the atomicMin
     unsigned delta;
     int l2_log, l3_log;
@@ -79,7 +80,7 @@ struct PlainParams {
 // warp of each CTA.
 struct Mirror {
     unsigned first, exit, pressure;
-    unsigned l3_reserve, l3_claim, l3_consumed;
+    unsigned l3_reserve, l3_claim, l3_consumed, l3_epoch;
     unsigned reserve[NB_MAX], claim[NB_MAX], consumed[NB_MAX];
 };
 
@@ -87,9 +88,11 @@ struct Mirror {
 // warp-uniform; c_lo/c_hi are lane-distributed (lane b: claim on ring b).
 struct WarpQ {
     int l1_head, l1_tail, l1_size;
+    int ob_n;  // records in the outbox (ring + OUTBOX_OFF)
     unsigned c_lo, c_hi;
     unsigned l3_lo, l3_hi;
     unsigned onfly;
+    unsigned l1_lim;  // winners at or above this distance skip L1 (bucket window)
     unsigned idle_ns;
     unsigned range_hit;
     unsigned long long pushed, l3_pushed, relaxed, improved;
@@ -198,6 +201,11 @@ __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool vali
         if (atomicCAS(slot, SENT, rec) != SENT) install_slow(p, slot, rec, q.deadline);
     }
     const unsigned l3m = __ballot_sync(FULL, valid && tgt == NB_MAX);
+    if (l3m) {
+        // Where the window goes when the next L3 epoch opens.
+        const unsigned dm = __reduce_min_sync(FULL, (valid && tgt == NB_MAX) ? d : 0xffffffffu);
+        if (lane == __ffs(l3m) - 1) atomicMin(p.ctlw + ctl::L3_MIN, dm);
+    }
     q.pushed += __popc(act);
     q.l3_pushed += __popc(l3m);
 }
@@ -207,8 +215,45 @@ __device__ __forceinline__ void push32(const PlainParams &p, WarpQ &q, bool vali
 // then spill everything to L2 when more than l1_spill records are held
 // (l1_queue.cu:332-350).  At most 32 records per call, so the 64-slot ring
 // never overflows.
+// Pushes the outbox's records 32 at a time (all of them when `all`, else
+// while 32 or more are held).  A warp empties it before it returns its read
+// credit, so the solve cannot end with records held here.
+__device__ __forceinline__ void outbox_flush(const PlainParams &p, WarpQ &q, uint2 *ring, bool all) {
+    const int lane = threadIdx.x & 31;
+    uint2 *ob = ring + OUTBOX_OFF;
+    while (q.ob_n >= 32 || (all && q.ob_n > 0)) {
+        const int k = q.ob_n < 32 ? q.ob_n : 32;
+        const int rest = q.ob_n - k;
+        const bool ok = lane < k;
+        uint2 it = make_uint2(0u, 0u), mv = make_uint2(0u, 0u);
+        if (ok) it = ob[lane];
+        if (lane < rest) mv = ob[k + lane];
+        __syncwarp();
+        if (lane < rest) ob[lane] = mv;
+        __syncwarp();
+        q.ob_n = rest;
+        push32(p, q, ok, it.x, it.y);
+    }
+}
+
 __device__ __forceinline__ void l1_write(const PlainParams &p, WarpQ &q, uint2 *ring, bool valid,
                                          unsigned v, unsigned d) {
+    // A winner beyond the bucket window goes to L2/L3, not to this warp's L1:
+    // following it here would let the warp's chain of relaxations run ahead
+    // of the window on distances that are not final yet, and the real
+    // frontier would redo that work later.  Such winners gather in the
+    // outbox and are pushed 32 at a time.
+    if (q.l1_lim != 0xffffffffu) {
+        const bool far = valid && d >= q.l1_lim;
+        const unsigned fm = __ballot_sync(FULL, far);
+        if (fm) {
+            if (far) ring[OUTBOX_OFF + q.ob_n + (int)__popc(fm & lanemask_lt())] = make_uint2(v, d);
+            __syncwarp();
+            q.ob_n += (int)__popc(fm);
+            if (q.ob_n >= 32) outbox_flush(p, q, ring, false);
+            valid = valid && !far;
+        }
+    }
     const unsigned vm = __ballot_sync(FULL, valid);
     if (!vm) return;
     const unsigned front_d =
@@ -313,6 +358,26 @@ __device__ __forceinline__ int read_ring(const PlainParams &p, WarpQ &q, volatil
     return t;
 }
 
+// Whether an L2 read could find anything: lane r looks at ring r (the urgent
+// ring or a bucket of the read window) in the CTA mirror -- unclaimed
+// reserved slots, or reserved slots inside this warp's own pending claim.
+// Costs one shared-memory read per lane and a vote, so an idle warp can
+// poll it instead of running the full read.
+__device__ __forceinline__ bool l2_has_work(const PlainParams &p, const WarpQ &q,
+                                            volatile Mirror &mir) {
+    const int lane = threadIdx.x & 31;
+    bool has = false;
+    if (lane <= p.nb) {
+        const unsigned rel = ((unsigned)lane + (unsigned)p.nb - mir.first % (unsigned)p.nb) %
+                             (unsigned)p.nb;
+        if (lane == p.nb || rel < (unsigned)p.bm) {
+            const unsigned res = mir.reserve[lane];
+            has = (int)(res - mir.claim[lane]) > 0 || (q.c_lo != q.c_hi && res != q.c_lo);
+        }
+    }
+    return __any_sync(FULL, has);
+}
+
 // L2 read (cu_delta_queue.cuh:272-428 with ml_queue.cu:238-307): urgent ring
 // first, then buckets first .. first+bucket_max-1, until min_read records.
 __device__ __forceinline__ int l2_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
@@ -326,19 +391,28 @@ __device__ __forceinline__ int l2_read(const PlainParams &p, WarpQ &q, volatile 
     return got;
 }
 
-// L3 read: only when every L2 ring is empty.  Takes up to 32 records and
-// moves `first` up to the smallest bucket among them.  Each taken record's
-// vertex bit is cleared and then the vertex's distance is read again: that
-// value covers every L3 push dropped while the record waited, and it is the
-// distance the record is relaxed with.
-__device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
-                                       uint2 *inb) {
+// L3 re-bucketing.  L3 holds records that did not fit the L2 window (beyond
+// it, or for a ring under pressure).  Relaxing them as they come out would
+// run a second, speculative wavefront far ahead of the real one; instead a
+// record goes back through push32 -- into the urgent ring below the window,
+// its bucket inside it, or L3 again beyond it -- so it is relaxed in bucket
+// order.  Reads happen in epochs: the controller opens one (sets L3_EPOCH to
+// the current L3 reserve count and moves `first` to the smallest distance
+// pushed to L3 since the last epoch) when everything outstanding is in L3,
+// and a warp with nothing else to do takes records from slots below the
+// epoch mark only, so each record is re-bucketed at most once per epoch.
+// Each taken record's vertex bit is cleared and then the vertex's distance is
+// read again: that value covers every L3 push dropped while the record
+// waited, and it is the distance the record goes back with.  Returns the
+// number of records taken (their read credit).
+__device__ __forceinline__ int l3_rebucket(const PlainParams &p, WarpQ &q, volatile Mirror &mir) {
     const int lane = threadIdx.x & 31;
     unsigned pending = 0;
     if (lane <= p.nb) pending = mir.reserve[lane] - mir.consumed[lane];
     if (__ballot_sync(FULL, pending != 0)) return 0;
+    const unsigned epoch = mir.l3_epoch;
     if (q.l3_lo == q.l3_hi) {
-        if ((int)(mir.l3_reserve - mir.l3_claim) <= 0) return 0;
+        if ((int)(epoch - mir.l3_claim) <= 0) return 0;
         unsigned nlo = 0;
         if (lane == 0) {
             nlo = atomicAdd(p.ctlw + ctl::L3_CLAIM, 32u);
@@ -347,7 +421,7 @@ __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile 
         q.l3_lo = __shfl_sync(FULL, nlo, 0);
         q.l3_hi = q.l3_lo + 32u;
     }
-    int ready = (int)(mir.l3_reserve - q.l3_lo);
+    int ready = (int)(min(epoch, mir.l3_reserve) - q.l3_lo);
     if (ready <= 0) return 0;
     if (ready > (int)(q.l3_hi - q.l3_lo)) ready = (int)(q.l3_hi - q.l3_lo);
     const unsigned s = q.l3_lo + lane;
@@ -360,24 +434,17 @@ __device__ __forceinline__ int l3_read(const PlainParams &p, WarpQ &q, volatile 
     const unsigned okm = __ballot_sync(FULL, ok);
     int take = (okm == FULL) ? 32 : (__ffs(~okm) - 1);
     if (take > ready) take = ready;
-    unsigned dmin = 0xffffffffu;
+    unsigned v = 0, cur = 0;
     if (lane < take) {
-        const unsigned v = rec_v(r);
+        v = rec_v(r);
         st_relaxed64(l3_slot(p, s), SENT);
         atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
         __threadfence();
-        const unsigned cur = min((unsigned)__ldcg(p.dist + v), rec_d(r));
-        inb[lane] = make_uint2(v, cur);
-        dmin = cur;
+        cur = min((unsigned)__ldcg(p.dist + v), rec_d(r));
     }
-    if (take > 0) {
-        for (int o = 16; o > 0; o >>= 1) dmin = min(dmin, __shfl_xor_sync(FULL, dmin, o));
-        if (lane == 0) {
-            atomicAdd(p.ctlw + ctl::L3_CONSUMED, (unsigned)take);
-            atomicMax(p.ctlw + ctl::FIRST, dmin / p.delta);
-        }
-    }
+    if (take > 0 && lane == 0) atomicAdd(p.ctlw + ctl::L3_CONSUMED, (unsigned)take);
     q.l3_lo += (unsigned)take;
+    push32(p, q, lane < take, v, cur);
     return take;
 }
 

@@ -124,6 +124,7 @@ int validate_config(const mlmq_config &c) {
     if (c.relax_unroll != 1 && c.relax_unroll != 2 && c.relax_unroll != 4) return MLMQ_ERR_ARG;
     if (c.relax_unroll > 1 && c.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
     if (c.vertex_tiles != 0 && c.vertex_tiles != 1) return MLMQ_ERR_ARG;
+    if (c.l1_ahead < 0) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -193,6 +194,7 @@ extern "C" int mlmq_config_default(mlmq_config *cfg) {
     cfg->l1_keep = 0;
     cfg->relax_precheck = 1;
     cfg->relax_unroll = 4;
+    cfg->l1_ahead = 4;
     cfg->vertex_tiles = 1;
     int rc = MLMQ_OK;
     bool have = false;
@@ -391,6 +393,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.l1_spill = s->cfg.l1_spill;
     p.l1_vector = s->cfg.queue_type == MLMQ_L1V_L2DQ;
     p.l1_keep = s->cfg.l1_keep;
+    p.l1_ahead = s->cfg.l1_ahead;
     p.precheck = s->cfg.relax_precheck;
     p.delta = (unsigned)s->cfg.delta;
     p.l2_log = s->l2_log;

@@ -154,6 +154,7 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     p.l1_spill = b->cfg.l1_spill;
     p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
     p.l1_keep = b->cfg.l1_keep;
+    p.l1_ahead = b->cfg.l1_ahead;
     p.precheck = b->cfg.relax_precheck;
     p.delta = (unsigned)b->cfg.delta;
     p.l2_log = b->l2_log;
@@ -352,6 +353,12 @@ extern "C" int mlmq_batch_query_status(const mlmq_batch *b, int q, unsigned *sta
         st->block = 32 * (b->workers + 1);
         st->status = c[ctl::STATUS];
     }
+    return MLMQ_OK;
+}
+
+extern "C" int mlmq_batch_control(const mlmq_batch *b, int q, unsigned *words, int count) {
+    if (!b || !words || q < 0 || q >= b->nq || count < 0 || count > CTL_STRIDE) return MLMQ_ERR_ARG;
+    std::memcpy(words, b->h_ctl + (size_t)q * CTL_STRIDE, sizeof(unsigned) * (size_t)count);
     return MLMQ_OK;
 }
 

@@ -43,6 +43,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
         const unsigned l3r = ld_relaxed(p.ctlw + ctl::L3_RESERVE);
         const unsigned l3c = ld_relaxed(p.ctlw + ctl::L3_CLAIM);
         const unsigned l3k = ld_relaxed(p.ctlw + ctl::L3_CONSUMED);
+        const unsigned l3e = ld_relaxed(p.ctlw + ctl::L3_EPOCH);
         unsigned ex = ld_relaxed(p.ctlw + ctl::EXIT);
         if (lane < rings) {
             mir.reserve[lane] = res;
@@ -55,6 +56,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
             mir.l3_reserve = l3r;
             mir.l3_claim = l3c;
             mir.l3_consumed = l3k;
+            mir.l3_epoch = l3e;
         }
         if (controller && !ex) {
             unsigned sum = lane < rings ? res : 0u;
@@ -70,15 +72,31 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
                     st_release(p.ctlw + ctl::EXIT, 1u);
                 }
                 ex = 1;
+            } else if (sum + l3r - credit == l3r - l3k && l3e != l3r) {
+                // Everything outstanding is unread in L3 (no L2 record, no
+                // warp holding work): open an L3 epoch.  The window moves up
+                // to the smallest distance pushed to L3 since the last one.
+                if (lane == 0) {
+                    const unsigned m = atomicExch(p.ctlw + ctl::L3_MIN, 0xffffffffu);
+                    if (m != 0xffffffffu) atomicMax(p.ctlw + ctl::FIRST, m / p.delta);
+                    st_release(p.ctlw + ctl::L3_EPOCH, l3r);
+                }
             } else {
-                if (wait != 0) {
-                    // Move `first` to the first non-empty bucket of the window.
+                // Urgent records (below the window) still to be read.
+                const unsigned urgent = __shfl_sync(FULL, res - con, p.nb);
+                if (wait != 0 && urgent == 0) {
+                    // Move `first` towards the first non-empty bucket of the
+                    // window, one bucket per step (as the reference's readers
+                    // do): a bucket whose records were all taken may still be
+                    // producing records in warps' L1 rings, and a window that
+                    // runs ahead of them turns their results into urgent
+                    // corrections of work already done.
                     const int b = (int)((first + (unsigned)lane) % (unsigned)p.nb);
                     const unsigned rb = __shfl_sync(FULL, res, b);
                     const unsigned cb = __shfl_sync(FULL, con, b);
                     const unsigned ne = __ballot_sync(FULL, lane < p.nb && rb != cb);
                     const int i0 = ne ? __ffs(ne) - 1 : 0;
-                    if (i0 > 0 && lane == 0) atomicMax(p.ctlw + ctl::FIRST, first + (unsigned)i0);
+                    if (i0 > 0 && lane == 0) atomicMax(p.ctlw + ctl::FIRST, first + 1u);
                 }
                 // Release bucket pressure once the ring has drained.
                 if (lane < p.nb && ((pres >> lane) & 1u) && res - con < cap8)
@@ -107,22 +125,38 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
     const int lane = threadIdx.x & 31;
     for (;;) {
         if (mir.exit) break;
+        if (p.l1_ahead) {
+            const unsigned long long lim =
+                ((unsigned long long)mir.first + (unsigned)p.l1_ahead) * p.delta;
+            q.l1_lim = lim < 0xffffffffull ? (unsigned)lim : 0xffffffffu;
+        }
         bool valid = false;
         unsigned v = 0, d = 0;
         if (q.l1_size > 0) {
             l1_read(q, ring, valid, v, d);
         } else {
+            if (q.ob_n) outbox_flush(p, q, ring, true);
             if (q.onfly) {
-                // L1 is empty: everything derived from the records read so far
-                // is reserved in L2/L3, so their credit may go back.
+                // L1 and the outbox are empty: everything derived from the
+                // records read so far is reserved in L2/L3, so their credit
+                // may go back.
                 __threadfence();
                 __syncwarp();
                 if (lane == 0) atomicAdd(p.ctlw + ctl::CREDIT, q.onfly);
                 q.onfly = 0;
             }
-            int got = l2_read(p, q, mir, inb);
-            if (got == 0) got = l3_read(p, q, mir, inb);
+            int got = l2_has_work(p, q, mir) ? l2_read(p, q, mir, inb) : 0;
             if (got == 0) {
+                // Nothing in L2: re-bucket L3 records if an epoch is open.
+                // Their credit is returned once L1 is empty, after the
+                // pushes that re-bucketed them.
+                const int moved = l3_rebucket(p, q, mir);
+                if (moved) {
+                    q.onfly += (unsigned)moved;
+                    q.idle_ns = 32;
+                    continue;
+                }
+
                 __nanosleep(q.idle_ns);
                 if (q.idle_ns < 256) q.idle_ns <<= 1;
                 continue;
@@ -168,6 +202,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         p.dist[p.src] = 0;
         *l2_slot(p, 0, 0u) = rec_pack((unsigned)p.src, 0u, 0u);
         p.ctlw[ctl::RESERVE + 0] = 1u;
+        p.ctlw[ctl::L3_MIN] = 0xffffffffu;
         p.ctlw[ctl::STATS + 2 * ctl::ST_PUSHED] = 1u;
     }
     if (!grid_barrier(p.ctlw, gsize, deadline)) return;
@@ -182,7 +217,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         mir.first = 0u;
         mir.exit = 0u;
         mir.pressure = 0u;
-        mir.l3_reserve = mir.l3_claim = mir.l3_consumed = 0u;
+        mir.l3_reserve = mir.l3_claim = mir.l3_consumed = mir.l3_epoch = 0u;
     }
     __syncthreads();
 
@@ -196,6 +231,8 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     int2 *stage = reinterpret_cast<int2 *>(inb + 32);
     WarpQ q;
     q.l1_head = q.l1_tail = q.l1_size = 0;
+    q.ob_n = 0;
+    q.l1_lim = 0xffffffffu;
     q.c_lo = q.c_hi = 0u;
     q.l3_lo = q.l3_hi = 0u;
     q.onfly = 0u;
