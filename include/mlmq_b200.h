@@ -97,6 +97,10 @@ typedef struct mlmq_config {
                             bucket is below first + l1_ahead, else it goes
                             to L2/L3 through the warp's outbox (default 4;
                             0: no limit, the reference's L1) */
+    int topup;           /* a warp that takes fewer than `topup` records from
+                            its L1 fills the rest of the warp from L2 in the
+                            same iteration (default 0 = off: it lengthens a
+                            single solve's critical path; batches use it) */
     int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
                             32-byte tile (up to 4 arcs inline, else its CSR
                             range); 0: row offsets, then arcs */
@@ -222,6 +226,8 @@ typedef struct mlmq_solve_stats {
     int grid;            /* persistent CTAs launched */
     int block;           /* threads per CTA */
     uint32_t status;     /* raw device status word */
+    uint64_t batches;    /* warp iterations that relaxed records */
+    uint64_t idle;       /* warp iterations that found nothing to do */
 } mlmq_solve_stats;
 int mlmq_solver_stats(mlmq_solver *s, mlmq_solve_stats *st);
 void mlmq_solver_destroy(mlmq_solver *s);

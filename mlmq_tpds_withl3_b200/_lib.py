@@ -61,7 +61,7 @@ class Config(ctypes.Structure):
         "queue_type", "delta", "work_blocks", "warps_per_block", "l2_batch",
         "bucket_num", "bucket_max", "min_read", "large_degree", "l1_spill",
         "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck",
-        "relax_unroll", "l1_ahead", "vertex_tiles")]
+        "relax_unroll", "l1_ahead", "topup", "vertex_tiles")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -77,7 +77,7 @@ class GraphInfo(ctypes.Structure):
 class SolveStats(ctypes.Structure):
     _fields_ = [("pushed", c_u64), ("l3_pushed", c_u64), ("relaxed", c_u64),
                 ("improved", c_u64), ("first_max", c_u32), ("grid", c_int),
-                ("block", c_int), ("status", c_u32)]
+                ("block", c_int), ("status", c_u32), ("batches", c_u64), ("idle", c_u64)]
 
 
 def _sig(name, res, *args):

@@ -121,17 +121,21 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
 
 def tune_batch(queries, max_vertices, candidates=None, base=None):
     """Times one batched launch of `queries` ([(DeviceGraph, source)]) per
-    candidate configuration (bucket width, L1 run-ahead bound, relaxation
-    rounds) and returns (config, report) for the fastest.  A batch is bound
-    by the GPU's total relaxation throughput rather than by one query's
-    chain of dependent hops, so its best setting differs from a single
-    solve's.  Every candidate gives the same exact distances."""
+    candidate configuration (bucket width, L1 top-up, run-ahead bound,
+    relaxation rounds) and returns (config, report) for the fastest.  A batch
+    keeps every warp busy, so it is bound by records relaxed per warp
+    iteration rather than by one query's chain of dependent hops, and its
+    best setting differs from a single solve's (the L1 top-up, which fills a
+    warp from L2 when its own L1 holds few records, pays off only here).
+    Every candidate gives the same exact distances."""
     from .batch import BatchSolver
     base = dict(base or {"warps_per_block": 8})
     if candidates is None:
-        candidates = [{"delta": d, "relax_unroll": u}
-                      for d in (50000, 100000, 200000) for u in (2, 4)]
-        candidates += [{"delta": 100000, "relax_unroll": 2, "l1_ahead": a} for a in (0, 2)]
+        candidates = [{"delta": d, "relax_unroll": 2, "topup": t}
+                      for d in (50000, 100000, 200000) for t in (8, 16, 32)]
+        candidates += [{"delta": 100000, "relax_unroll": 4, "topup": 16},
+                       {"delta": 100000, "relax_unroll": 2, "topup": 16, "l1_ahead": 8},
+                       {"delta": 100000, "relax_unroll": 2}]
     results = []
     for over in candidates:
         b = BatchSolver(len(queries), max_vertices, {**base, **over})

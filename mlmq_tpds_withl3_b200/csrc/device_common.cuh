@@ -17,10 +17,13 @@ constexpr unsigned long long SENT = ~0ull;  // empty ring slot
 constexpr int TILE_ARCS = 4;
 constexpr int TILE_CSR = -2;
 // 8-byte shared-memory slots per worker warp: L1 ring, L2/L3 read buffer,
-// staged tile arcs, outbox of records bound for L2/L3.
+// staged tile arcs, outbox of records bound for L2/L3, winners of the
+// relaxation rounds in flight (at most 4 rounds of 32).
 constexpr int OUTBOX_CAP = 64;
 constexpr int OUTBOX_OFF = L1_CAP + 32 + 32 * TILE_ARCS;
-constexpr int WARP_SMEM_SLOTS = OUTBOX_OFF + OUTBOX_CAP;
+constexpr int WINBUF_CAP = 128;
+constexpr int WINBUF_OFF = OUTBOX_OFF + OUTBOX_CAP;
+constexpr int WARP_SMEM_SLOTS = WINBUF_OFF + WINBUF_CAP;
 
 // ---- control block: 32-bit words, one 128-byte line per group ------------
 namespace ctl {
@@ -42,7 +45,7 @@ constexpr int L3_CLAIM = 192;
 constexpr int L3_CONSUMED = 224;
 constexpr int STATS = 256;    // u64 counters (word offset, 8-byte aligned)
 constexpr int ST_PUSHED = 0, ST_L3_PUSHED = 1, ST_RELAXED = 2, ST_IMPROVED = 3, ST_FIRST_MAX = 4,
-              ST_N = 8;
+              ST_BATCHES = 5, ST_IDLE = 6, ST_N = 8;
 constexpr int WORDS = STATS + 2 * ST_N;  // 272 words
 }  // namespace ctl
 

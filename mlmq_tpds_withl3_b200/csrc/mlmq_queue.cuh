@@ -69,6 +69,7 @@ struct PlainParams {
     int nb, bm, batch, min_read, large, l1_spill, l1_vector;
     int l1_keep;   // records kept at the L1 front when it spills (0: spill all)
     int l1_ahead;  // buckets past `first` a winner may be to stay in L1 (0: no limit)
+    int topup;     // fewer than this many L1 records: fill the warp from L2 too
     int precheck;  // read dist[dst] before the atomicMin
     unsigned delta;
     int l2_log, l3_log;
@@ -96,6 +97,7 @@ struct WarpQ {
     unsigned idle_ns;
     unsigned range_hit;
     unsigned long long pushed, l3_pushed, relaxed, improved;
+    unsigned batches, idle;  // warp iterations with records / without (warp-uniform)
     unsigned long long deadline;
 };
 
@@ -306,13 +308,13 @@ __device__ __forceinline__ void l1_read(WarpQ &q, const uint2 *ring, bool &valid
 // Takes the readable prefix of this warp's claim on L2 ring `ring` into
 // inb[got...]; returns the number taken.
 __device__ __forceinline__ int take_claim(const PlainParams &p, volatile Mirror &mir, int ring,
-                                          unsigned &lo, unsigned hi, uint2 *inb, int got) {
+                                          unsigned &lo, unsigned hi, uint2 *inb, int got, int room) {
     const int lane = threadIdx.x & 31;
     const unsigned res = mir.reserve[ring];
     int ready = (int)(res - lo);
     if (ready <= 0) return 0;
     if (ready > (int)(hi - lo)) ready = (int)(hi - lo);
-    if (ready > 32 - got) ready = 32 - got;
+    if (ready > room - got) ready = room - got;
     unsigned long long r = SENT;
     bool ok = false;
     const unsigned s = lo + lane;
@@ -335,13 +337,13 @@ __device__ __forceinline__ int take_claim(const PlainParams &p, volatile Mirror 
 // One ring of the read window: continue a pending claim or make a new one
 // (only when the mirror shows unclaimed reserved slots), then take records.
 __device__ __forceinline__ int read_ring(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
-                                         int ring, uint2 *inb, int got) {
+                                         int ring, uint2 *inb, int got, int room) {
     const int lane = threadIdx.x & 31;
     unsigned lo = __shfl_sync(FULL, q.c_lo, ring);
     unsigned hi = __shfl_sync(FULL, q.c_hi, ring);
     if (lo == hi) {
         if ((int)(mir.reserve[ring] - mir.claim[ring]) <= 0) return 0;
-        if (got + p.batch > 32) return 0;
+        if (got + p.batch > room) return 0;
         unsigned nlo = 0;
         if (lane == 0) {
             nlo = atomicAdd(p.ctlw + ctl::CLAIM + ring, (unsigned)p.batch);
@@ -350,7 +352,7 @@ __device__ __forceinline__ int read_ring(const PlainParams &p, WarpQ &q, volatil
         lo = __shfl_sync(FULL, nlo, 0);
         hi = lo + (unsigned)p.batch;
     }
-    const int t = take_claim(p, mir, ring, lo, hi, inb, got);
+    const int t = take_claim(p, mir, ring, lo, hi, inb, got, room);
     if (lane == ring) {
         q.c_lo = lo;
         q.c_hi = hi;
@@ -379,14 +381,15 @@ __device__ __forceinline__ bool l2_has_work(const PlainParams &p, const WarpQ &q
 }
 
 // L2 read (cu_delta_queue.cuh:272-428 with ml_queue.cu:238-307): urgent ring
-// first, then buckets first .. first+bucket_max-1, until min_read records.
+// first, then buckets first .. first+bucket_max-1, until `want` records (at
+// most `room`) are in inb.
 __device__ __forceinline__ int l2_read(const PlainParams &p, WarpQ &q, volatile Mirror &mir,
-                                       uint2 *inb) {
-    int got = read_ring(p, q, mir, p.nb, inb, 0);
+                                       uint2 *inb, int room, int want) {
+    int got = read_ring(p, q, mir, p.nb, inb, 0, room);
     const unsigned f = mir.first;
-    for (int i = 0; i < p.bm && got < p.min_read; i++) {
+    for (int i = 0; i < p.bm && got < want; i++) {
         const int b = (int)((f + (unsigned)i) % (unsigned)p.nb);
-        got += read_ring(p, q, mir, b, inb, got);
+        got += read_ring(p, q, mir, b, inb, got, room);
     }
     return got;
 }
@@ -500,13 +503,29 @@ __device__ __forceinline__ void relax_known(const PlainParams &p, WarpQ &q, uint
             }
         }
     }
+    // Winners of all rounds are compacted into the warp's winner buffer and
+    // go to L1 32 at a time: full warps, and one copy of the L1 code.
+    const int lane = threadIdx.x & 31;
+    uint2 *wb = ring + WINBUF_OFF;
+    int nw = 0;
 #pragma unroll
     for (int k = 0; k < K; k++) {
         if (k < rounds) {
+            const unsigned m = __ballot_sync(FULL, win[k]);
+            if (win[k]) wb[nw + (int)__popc(m & lanemask_lt())] = make_uint2(dst[k], nd[k]);
+            nw += (int)__popc(m);
             q.improved += win[k];
-            l1_write(p, q, ring, win[k], dst[k], nd[k]);
         }
     }
+    __syncwarp();
+#pragma unroll 1
+    for (int c = 0; c < nw; c += 32) {
+        const bool ok = c + lane < nw;
+        uint2 it = make_uint2(0u, 0u);
+        if (ok) it = wb[c + lane];
+        l1_write(p, q, ring, ok, it.x, it.y);
+    }
+    __syncwarp();
 }
 
 // Loads the arcs of K lane-distributed rounds (round k: this lane's arc ai[k]

@@ -162,6 +162,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.l1_vector = cfg.queue_type == MLMQ_L1V_L2DQ;
     p.l1_keep = cfg.l1_keep;
     p.l1_ahead = cfg.l1_ahead;
+    p.topup = cfg.topup;
     p.precheck = cfg.relax_precheck;
     p.delta = (unsigned)cfg.delta;
     p.l2_log = NA_L2_LOG;

@@ -125,6 +125,7 @@ int validate_config(const mlmq_config &c) {
     if (c.relax_unroll > 1 && c.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
     if (c.vertex_tiles != 0 && c.vertex_tiles != 1) return MLMQ_ERR_ARG;
     if (c.l1_ahead < 0) return MLMQ_ERR_ARG;
+    if (c.topup < 0 || c.topup > 32) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -394,6 +395,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.l1_vector = s->cfg.queue_type == MLMQ_L1V_L2DQ;
     p.l1_keep = s->cfg.l1_keep;
     p.l1_ahead = s->cfg.l1_ahead;
+    p.topup = s->cfg.topup;
     p.precheck = s->cfg.relax_precheck;
     p.delta = (unsigned)s->cfg.delta;
     p.l2_log = s->l2_log;
@@ -455,6 +457,8 @@ extern "C" int mlmq_solver_stats(mlmq_solver *s, mlmq_solve_stats *st) {
     st->relaxed = c[ctl::ST_RELAXED];
     st->improved = c[ctl::ST_IMPROVED];
     st->first_max = (uint32_t)c[ctl::ST_FIRST_MAX];
+    st->batches = c[ctl::ST_BATCHES];
+    st->idle = c[ctl::ST_IDLE];
     st->grid = s->grid;
     st->block = 32 * (s->workers + 1);
     st->status = s->h_ctl[ctl::STATUS];

@@ -155,6 +155,7 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     p.l1_vector = b->cfg.queue_type == MLMQ_L1V_L2DQ;
     p.l1_keep = b->cfg.l1_keep;
     p.l1_ahead = b->cfg.l1_ahead;
+    p.topup = b->cfg.topup;
     p.precheck = b->cfg.relax_precheck;
     p.delta = (unsigned)b->cfg.delta;
     p.l2_log = b->l2_log;
@@ -349,6 +350,8 @@ extern "C" int mlmq_batch_query_status(const mlmq_batch *b, int q, unsigned *sta
         st->relaxed = u[ctl::ST_RELAXED];
         st->improved = u[ctl::ST_IMPROVED];
         st->first_max = (uint32_t)u[ctl::ST_FIRST_MAX];
+        st->batches = u[ctl::ST_BATCHES];
+        st->idle = u[ctl::ST_IDLE];
         st->grid = b->grid;
         st->block = 32 * (b->workers + 1);
         st->status = c[ctl::STATUS];

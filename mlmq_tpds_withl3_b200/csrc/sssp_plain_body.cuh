@@ -133,7 +133,24 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
         bool valid = false;
         unsigned v = 0, d = 0;
         if (q.l1_size > 0) {
+            const int k = q.l1_size < 32 ? q.l1_size : 32;
             l1_read(q, ring, valid, v, d);
+            if (k < p.topup && l2_has_work(p, q, mir)) {
+                // Few records in L1: fill the rest of the warp from the L2
+                // window, so an iteration relaxes a full warp of records.
+                const int got = l2_read(p, q, mir, inb, 32 - k, 32 - k);
+                if (got) {
+                    q.onfly += (unsigned)got;
+                    __syncwarp();
+                    if (lane >= k && lane < k + got) {
+                        const uint2 it = inb[lane - k];
+                        valid = true;
+                        v = it.x;
+                        d = it.y;
+                    }
+                    __syncwarp();
+                }
+            }
         } else {
             if (q.ob_n) outbox_flush(p, q, ring, true);
             if (q.onfly) {
@@ -145,7 +162,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
                 if (lane == 0) atomicAdd(p.ctlw + ctl::CREDIT, q.onfly);
                 q.onfly = 0;
             }
-            int got = l2_has_work(p, q, mir) ? l2_read(p, q, mir, inb) : 0;
+            int got = l2_has_work(p, q, mir) ? l2_read(p, q, mir, inb, 32, p.min_read) : 0;
             if (got == 0) {
                 // Nothing in L2: re-bucket L3 records if an epoch is open.
                 // Their credit is returned once L1 is empty, after the
@@ -157,6 +174,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
                     continue;
                 }
 
+                q.idle++;
                 __nanosleep(q.idle_ns);
                 if (q.idle_ns < 256) q.idle_ns <<= 1;
                 continue;
@@ -172,6 +190,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
             }
             __syncwarp();
         }
+        q.batches++;
         relax_batch<Arcs, K>(p, q, ring, stage, valid, v, d);
     }
 }
@@ -239,6 +258,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     q.idle_ns = 32u;
     q.range_hit = 0u;
     q.pushed = q.l3_pushed = q.relaxed = q.improved = 0ull;
+    q.batches = q.idle = 0u;
     q.deadline = deadline;
 
     worker_loop<Arcs, K>(p, mir, ring, inb, stage, q);
@@ -257,6 +277,8 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         atomicAdd(st + ctl::ST_L3_PUSHED, q.l3_pushed);
         atomicAdd(st + ctl::ST_RELAXED, relaxed);
         atomicAdd(st + ctl::ST_IMPROVED, improved);
+        atomicAdd(st + ctl::ST_BATCHES, (unsigned long long)q.batches);
+        atomicAdd(st + ctl::ST_IDLE, (unsigned long long)q.idle);
         if (range) atomicOr(p.ctlw + ctl::STATUS, ST_RANGE);
         atomicMax(st + ctl::ST_FIRST_MAX, (unsigned long long)ld_relaxed(p.ctlw + ctl::FIRST));
     }

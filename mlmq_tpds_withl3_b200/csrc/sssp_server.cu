@@ -355,6 +355,7 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         b.l1_vector = cfg.queue_type == MLMQ_L1V_L2DQ;
         b.l1_keep = cfg.l1_keep;
         b.l1_ahead = cfg.l1_ahead;
+        b.topup = cfg.topup;
         b.precheck = cfg.relax_precheck;
         b.delta = (unsigned)cfg.delta;
         b.l2_log = sv->l2_log;

@@ -79,6 +79,9 @@ def test_c1_grid512_bit_exact():
     {"relax_unroll": 1, "warps_per_block": 31},
     {"vertex_tiles": 0},
     {"vertex_tiles": 0, "relax_precheck": 0, "relax_unroll": 1},
+    {"topup": 32},
+    {"topup": 16, "l1_ahead": 0, "min_read": 1},
+    {"l1_ahead": 1, "delta": 2000},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
