@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--max-queries", type=int, default=4000)
     ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
+    ap.add_argument("--side", type=int, default=0,
+                    help="c4: grid side instead of 4896 (small cases for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
@@ -379,7 +381,10 @@ def run_batched(args):
     import oracle_lib
     from mlmq_tpds_withl3_b200 import BatchSolver, DeviceGraph, Solver, default_config
 
-    g, srcs = load_workload("c4", args.sources)
+    from mlmq_tpds_withl3_b200 import workloads
+    g, srcs = workloads.c4(side=args.side) if args.side else workloads.c4()
+    if args.sources:
+        srcs = srcs[:args.sources]
     dg = DeviceGraph.upload(g)
     queries = [(dg, s) for s in srcs]
     tune_report = None
@@ -449,7 +454,9 @@ def run_batched(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD_TEXT["c4"], "n": g.n, "m": g.m, "sources": len(srcs),
+        "config": {"workload": WORKLOAD_TEXT["c4"] if not args.side else
+                   f"batched: {len(srcs)} sources on a {args.side}x{args.side} grid (profiling case)",
+                   "n": g.n, "m": g.m, "sources": len(srcs),
                    "delta": bcfg.delta, "warps_per_block": bcfg.warps_per_block,
                    "l1_ahead": bcfg.l1_ahead, "relax_unroll": bcfg.relax_unroll,
                    "grid": batch.grid,
@@ -496,7 +503,24 @@ def run_served(args):
     dgs = [DeviceGraph.upload(hgs[k]) for k in names]
     ns = [hgs[k].n for k in names]
     max_n = max(ns)
-    cfg = default_config(delta=200000, warps_per_block=8)
+    tune_report = None
+    cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2)
+    knobs = None
+    if not args.no_tune:
+        # Each resident graph gets the per-query settings (delta, topup,
+        # run-ahead bound) that were fastest on a batched launch of 64 of its
+        # own queries; the server passes them with every query on that graph.
+        from mlmq_tpds_withl3_b200 import autotune
+        cands = [{"delta": d, "topup": t} for d in (50000, 100000, 200000) for t in (16, 32)]
+        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0}]
+        knobs, tune_report = [], {}
+        for i, dg in enumerate(dgs):
+            rng = np.random.default_rng(70 + i)
+            qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
+            kc, rep = autotune.tune_batch(qs, ns[i], candidates=cands,
+                                          base={"warps_per_block": 8, "relax_unroll": 2})
+            knobs.append(kc)
+            tune_report[names[i]] = rep["config"]
     sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900)
     pool = PinnedPool(sv.slots, max_n)
     rates = [float(r) for r in args.rates.split(",")]
@@ -506,7 +530,7 @@ def run_served(args):
         count = int(min(max(30, rate * args.serve_seconds), args.max_queries))
         sched = poisson_schedule(rate, count, ns, seed=100 + ri)
         keep = (lambda i: i % 40 == 0)
-        recs = serve_poisson(sv, dgs, sched, keep=keep, pool=pool, timeout_s=600)
+        recs = serve_poisson(sv, dgs, sched, keep=keep, pool=pool, timeout_s=600, knobs=knobs)
         s = summarize(recs, names)
         s["rate"] = rate
         sweep.append(s)
@@ -524,7 +548,15 @@ def run_served(args):
     for (ri, i), r in sample.items():
         gi = r["graph"]
         if gi not in solvers:
-            solvers[gi] = Solver(dgs[gi], cfg={"delta": 200000})
+            # Each graph's back-to-back baseline runs its own tuned
+            # single-solve configuration.
+            pc = default_config(delta=200000)
+            if not args.no_tune:
+                from mlmq_tpds_withl3_b200 import autotune
+                hg = hgs[names[gi]]
+                probe = [int(x) for x in np.random.default_rng(gi).integers(0, hg.n, 2)]
+                pc, _ = autotune.tune(dgs[gi], hg, probe, kind=f"c5-{names[gi]}", use_cache=False)
+            solvers[gi] = Solver(dgs[gi], pc)
         s = solvers[gi]
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -548,7 +580,9 @@ def run_served(args):
         "config": {"workload": "served: grids 2^16..2^24 + R-MAT 18/20/22 resident; Poisson "
                                "arrivals, graph and source uniform per query",
                    "graphs": {k: {"n": hgs[k].n, "m": hgs[k].m} for k in names},
-                   "slots": sv.slots, "grid": sv.grid, "delta": 200000, "rates": rates},
+                   "slots": sv.slots, "grid": sv.grid, "delta": cfg.delta,
+                   "warps_per_block": cfg.warps_per_block, "relax_unroll": cfg.relax_unroll,
+                   "l1_ahead": cfg.l1_ahead, "rates": rates},
         "sweep": sweep,
         "latency_ms": {"p50": top["p50_ms"], "p99": top["p99_ms"], "at_rate": top["rate"]},
         "plain_back_to_back": {"qps": plain_qps, "queries": len(plain_ms),
@@ -559,6 +593,8 @@ def run_served(args):
         "correct": bool(correct),
         "checked_alone_vs_mix": len(sample),
     }
+    if tune_report:
+        line["autotune"] = {"per_graph_query_settings": tune_report}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

@@ -288,6 +288,12 @@ int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block);
  * stay valid until the ticket is reported by mlmq_server_poll. */
 int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
                        uint64_t *ticket);
+/* As mlmq_server_submit, with this query's delta, topup, l1_ahead and
+ * bucket_max taken from *knobs (the other fields are fixed per server and
+ * ignored; NULL = the server's configuration), so queries on graphs of
+ * different shapes can each run their own tuned settings in one server. */
+int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int src,
+                           const mlmq_config *knobs, int *h_out, uint64_t *ticket);
 /* Advances finished queries (result copy-out) and reports up to `max`
  * completed tickets with their MLMQ_ERR_* status. */
 int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max, int *count);

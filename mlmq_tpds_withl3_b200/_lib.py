@@ -140,6 +140,8 @@ _sig("mlmq_server_create", c_int, c_int, c_int, ctypes.POINTER(Config), c_int,
 _sig("mlmq_server_info", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
      ctypes.POINTER(c_int))
 _sig("mlmq_server_submit", c_int, c_vp, c_vp, c_int, c_vp, ctypes.POINTER(c_u64))
+_sig("mlmq_server_submit_cfg", c_int, c_vp, c_vp, c_int, ctypes.POINTER(Config), c_vp,
+     ctypes.POINTER(c_u64))
 _sig("mlmq_server_poll", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_int), c_int,
      ctypes.POINTER(c_int))
 _sig("mlmq_server_busy_slots", c_int, c_vp, ctypes.POINTER(c_int))

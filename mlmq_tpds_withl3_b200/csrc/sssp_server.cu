@@ -38,7 +38,8 @@ namespace {
 constexpr int SRV_CTL_STRIDE = 512;  // words per slot control block
 // Words of the slot control block used by the server around a solve (the
 // solve itself uses words below ctl::WORDS).
-constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs, tiles (2 words each), n, src
+constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs, tiles (2 words each),
+                                  // n, src, delta, topup, l1_ahead, bucket_max
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_BAR_COUNT = 488;
@@ -59,6 +60,9 @@ struct alignas(64) SlotCommand {
     const int4 *tiles;
     int n;
     int src;
+    // per-query settings (the server's configuration unless overridden)
+    unsigned delta;
+    int topup, l1_ahead, bm;
 };
 // Host-mapped completion, one per slot, written by the device.
 struct alignas(64) SlotCompletion {
@@ -152,6 +156,10 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                         const unsigned long long tiles = (unsigned long long)sp.cmd[s].tiles;
                         c[SRV_CMD + 6] = (unsigned)tiles;
                         c[SRV_CMD + 7] = (unsigned)(tiles >> 32);
+                        c[SRV_CMD + 8] = sp.cmd[s].delta;
+                        c[SRV_CMD + 9] = (unsigned)sp.cmd[s].topup;
+                        c[SRV_CMD + 10] = (unsigned)sp.cmd[s].l1_ahead;
+                        c[SRV_CMD + 11] = (unsigned)sp.cmd[s].bm;
                         __threadfence();
                         // publish the sequence number (low 32 bits) to the group
                         st_release(c + SRV_GO, (unsigned)q);
@@ -185,6 +193,10 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         p.row = (const int *)(((unsigned long long)cmd[1] << 32) | cmd[0]);
         p.arcs = (const int2 *)(((unsigned long long)cmd[3] << 32) | cmd[2]);
         p.tiles = (const int4 *)(((unsigned long long)cmd[7] << 32) | cmd[6]);
+        p.delta = cmd[8];
+        p.topup = (int)cmd[9];
+        p.l1_ahead = (int)cmd[10];
+        p.bm = (int)cmd[11];
         p.n = (int)cmd[4];
         p.src = (int)cmd[5];
         p.dist = sp.dist + (size_t)s * sp.max_n;
@@ -411,11 +423,15 @@ extern "C" int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, in
     return MLMQ_OK;
 }
 
-extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
-                                  uint64_t *ticket) {
+extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int src,
+                                      const mlmq_config *knobs, int *h_out, uint64_t *ticket) {
     if (!sv || !g || !h_out || !ticket || src < 0 || src >= g->n || g->n > sv->max_n)
         return MLMQ_ERR_ARG;
     if (g->device != sv->device) return MLMQ_ERR_ARG;
+    const mlmq_config &k = knobs ? *knobs : sv->cfg;
+    if (k.delta < 1 || k.topup < 0 || k.topup > 32 || k.l1_ahead < 0 || k.bucket_max < 1 ||
+        k.bucket_max > sv->cfg.bucket_num)
+        return MLMQ_ERR_ARG;
     std::lock_guard<std::mutex> lk(sv->mu);
     if (!sv->running) return MLMQ_ERR_STATE;
     int free_slot = -1;
@@ -432,6 +448,10 @@ extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src,
     cmd.tiles = sv->cfg.vertex_tiles ? g->d_tiles : nullptr;
     cmd.n = g->n;
     cmd.src = src;
+    cmd.delta = (unsigned)k.delta;
+    cmd.topup = k.topup;
+    cmd.l1_ahead = k.l1_ahead;
+    cmd.bm = k.bucket_max;
     std::atomic_thread_fence(std::memory_order_release);
     sl.seq++;
     sl.busy = true;
@@ -442,6 +462,11 @@ extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src,
     cmd.seq = sl.seq;  // published last
     *ticket = sl.ticket;
     return MLMQ_OK;
+}
+
+extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
+                                  uint64_t *ticket) {
+    return mlmq_server_submit_cfg(sv, g, src, nullptr, h_out, ticket);
 }
 
 // Moves finished solves to the copy stream and retires finished copies.

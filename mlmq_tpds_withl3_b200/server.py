@@ -36,13 +36,18 @@ class Server:
         self._tk = (ctypes.c_uint64 * 256)()
         self._st = (ctypes.c_int * 256)()
 
-    def submit(self, dgraph, src, out):
+    def submit(self, dgraph, src, out, knobs=None):
         """Returns a ticket, or None when every slot is busy.  `out` must be a
         host int32 buffer of dgraph.n entries (pinned for asynchronous copy)
-        that stays alive until the ticket completes."""
+        that stays alive until the ticket completes.  `knobs` (a Config)
+        gives this query its own delta, topup, l1_ahead and bucket_max."""
         t = ctypes.c_uint64()
         ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
-        rc = lib.mlmq_server_submit(self._h, dgraph.handle, int(src), ptr, ctypes.byref(t))
+        if knobs is not None:
+            rc = lib.mlmq_server_submit_cfg(self._h, dgraph.handle, int(src), ctypes.byref(knobs),
+                                            ptr, ctypes.byref(t))
+        else:
+            rc = lib.mlmq_server_submit(self._h, dgraph.handle, int(src), ptr, ctypes.byref(t))
         if rc == MLMQ_ERR_BUSY:
             return None
         check(rc, "mlmq_server_submit")
@@ -92,10 +97,11 @@ def poisson_schedule(rate, count, graphs_n, seed=1):
     return list(zip(t.tolist(), gi.tolist(), src))
 
 
-def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0):
+def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0, knobs=None):
     """Runs the schedule against the server.  Returns a list of dicts
     (arrival, start, finish, latency_s, graph, src, status[, dist]) in
-    schedule order; `keep(i)` selects the queries whose distances are kept."""
+    schedule order; `keep(i)` selects the queries whose distances are kept;
+    `knobs[graph index]` (optional) is that graph's per-query Config."""
     pool = pool or PinnedPool(server.slots, max(g.n for g in dgraphs))
     pending = deque(range(len(schedule)))
     inflight = {}
@@ -112,7 +118,8 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
             if buf is None:
                 break
             _, gi, src = schedule[i]
-            tk = server.submit(dgraphs[gi], src, buf)
+            tk = server.submit(dgraphs[gi], src, buf,
+                               knobs[gi] if knobs is not None else None)
             if tk is None:
                 pool.put(buf)
                 break

@@ -39,6 +39,32 @@ def test_served_results_equal_oracle_and_alone():
     assert s["errors"] == 0 and s["queries"] == 80
 
 
+def test_per_query_settings_give_the_same_result():
+    """Queries submitted with their own delta / topup / run-ahead bound /
+    read window return the same distances as the oracle."""
+    from mlmq_tpds_withl3_b200 import default_config
+    g = HostGraph.grid(200, 180, seed=46)
+    dg = DeviceGraph.upload(g)
+    sv = Server(slots=4, max_vertices=g.n, lifetime_s=60)
+    import torch
+    knobs = [default_config(delta=5000, topup=32, l1_ahead=1, bucket_max=2),
+             default_config(delta=400000, topup=0, l1_ahead=0, bucket_max=8), None]
+    bufs = [torch.empty(g.n, dtype=torch.int32, pin_memory=True) for _ in knobs]
+    tks = [sv.submit(dg, 9, b, k) for b, k in zip(bufs, knobs)]
+    assert all(t is not None for t in tks)
+    done = {}
+    import time
+    t0 = time.time()
+    while len(done) < len(tks) and time.time() - t0 < 30:
+        for tk, st in sv.poll():
+            done[tk] = st
+    sv.close()
+    assert all(done.get(t) == 0 for t in tks)
+    ref, _ = oracle_lib.sssp_i32(g, 9)
+    for b in bufs:
+        assert np.array_equal(b.numpy(), ref)
+
+
 def test_server_busy_and_stop():
     g = HostGraph.grid(64, 64, seed=45)
     dg = DeviceGraph.upload(g)
