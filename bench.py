@@ -392,8 +392,8 @@ def run_batched(args):
         bcfg = default_config(delta=200000, warps_per_block=8)
     else:
         from mlmq_tpds_withl3_b200 import autotune
-        bcfg, tune_report = autotune.tune_batch(queries, g.n)
-    batch = BatchSolver(len(srcs), g.n, bcfg)
+        bcfg, tune_report = autotune.tune_batch(queries, dg.slots)
+    batch = BatchSolver(len(srcs), dg.slots, bcfg)
     stream = torch.cuda.Stream()
 
     # Correctness: oracle on a few sources, the plain solver on every source.
@@ -502,7 +502,7 @@ def run_served(args):
     names = list(hgs)
     dgs = [DeviceGraph.upload(hgs[k]) for k in names]
     ns = [hgs[k].n for k in names]
-    max_n = max(ns)
+    max_n = max(dg.slots for dg in dgs)
     tune_report = None
     cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2)
     knobs = None
@@ -517,7 +517,7 @@ def run_served(args):
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
-            kc, rep = autotune.tune_batch(qs, ns[i], candidates=cands,
+            kc, rep = autotune.tune_batch(qs, dg.slots, candidates=cands,
                                           base={"warps_per_block": 8, "relax_unroll": 2})
             knobs.append(kc)
             tune_report[names[i]] = rep["config"]

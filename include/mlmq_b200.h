@@ -199,6 +199,11 @@ int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const in
 int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
                            const int *d_w, mlmq_graph **out);
 int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m);
+/* Vertices of more than 1024 arcs are relaxed as pieces of at most 512 arcs
+ * that different warps take in parallel; each piece is a virtual vertex id
+ * after the graph's n.  A batch or server solving this graph needs
+ * max_vertices >= n + pieces. */
+int mlmq_graph_pieces(const mlmq_graph *g, int *pieces);
 void mlmq_graph_free(mlmq_graph *g);
 
 /* A solver owns one distance array and one queue workspace on the device
@@ -247,6 +252,7 @@ int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int 
 typedef struct mlmq_batch mlmq_batch;
 /* cfg may be NULL: mlmq_config_default() with 8 worker warps per CTA.
  * Per-slot rings default to 2^18 slots (L2) and 2^20 slots (L3). */
+/* max_vertices bounds n + mlmq_graph_pieces() of every graph a launch uses. */
 int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_config *cfg,
                       mlmq_batch **out);
 int mlmq_batch_info(const mlmq_batch *b, int *grid, int *block, int *max_queries);

@@ -16,6 +16,13 @@ constexpr unsigned long long SENT = ~0ull;  // empty ring slot
 // slots dst = -1), or {TILE_CSR, first arc, degree, ...} for higher degree.
 constexpr int TILE_ARCS = 4;
 constexpr int TILE_CSR = -2;
+// A vertex of more than SPLIT_MIN arcs is relaxed as pieces of at most
+// PIECE_ARCS arcs.  Piece k of the graph is a virtual vertex id n + k with
+// tile {TILE_CSR, first arc, arcs, owner}; the heavy vertex's own tile is
+// {TILE_SPLIT, first piece id, pieces, degree}.
+constexpr int TILE_SPLIT = -3;
+constexpr int SPLIT_MIN = 1024;
+constexpr int PIECE_ARCS = 512;
 // 8-byte shared-memory slots per worker warp: L1 ring, L2/L3 read buffer,
 // staged tile arcs, outbox of records bound for L2/L3, winners of the
 // relaxation rounds in flight (at most 4 rounds of 32).

@@ -55,6 +55,7 @@ namespace mlmq {
 
 struct PlainParams {
     int n;
+    int nslots;  // n + split-vertex pieces (ids n .. nslots-1 are pieces)
     const int *__restrict__ row;
     const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
     const int4 *__restrict__ tiles; // 2 per vertex, or null: read row offsets instead
@@ -443,7 +444,9 @@ __device__ __forceinline__ int l3_rebucket(const PlainParams &p, WarpQ &q, volat
         st_relaxed64(l3_slot(p, s), SENT);
         atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
         __threadfence();
-        cur = min((unsigned)__ldcg(p.dist + v), rec_d(r));
+        // A piece has no distance of its own: its owner's stands for it.
+        const unsigned dv = v < (unsigned)p.n ? v : (unsigned)__ldg(p.tiles + 2 * (size_t)v).w;
+        cur = min((unsigned)__ldcg(p.dist + dv), rec_d(r));
     }
     if (take > 0 && lane == 0) atomicAdd(p.ctlw + ctl::L3_CONSUMED, (unsigned)take);
     q.l3_lo += (unsigned)take;
@@ -549,6 +552,36 @@ __device__ __forceinline__ void relax_rounds(const PlainParams &p, WarpQ &q, uin
     relax_known<K>(p, q, ring, ok, dst, nd, rounds);
 }
 
+// A heavy vertex is not relaxed by the warp that read it: one record per
+// piece, at the vertex's distance, goes to L2, where any warp may take it.
+// Lane-distributed as arcs are: an exclusive prefix sum of piece counts and
+// a shuffle search for the owner lane of each piece.
+__device__ __forceinline__ void push_pieces(const PlainParams &p, WarpQ &q, int np, int first,
+                                            unsigned d) {
+    const int lane = threadIdx.x & 31;
+    int incl = np;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const int off = incl - np;
+    for (int e0 = 0; e0 < total; e0 += 32) {
+        const int e = e0 + lane;
+        int j = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const int oc = __shfl_sync(FULL, off, j + s);
+            if (oc <= e) j += s;
+        }
+        const int fj = __shfl_sync(FULL, first, j);
+        const int oj = __shfl_sync(FULL, off, j);
+        const unsigned dj = __shfl_sync(FULL, d, j);
+        push32(p, q, e < total, (unsigned)(fj + (e - oj)), dj);
+    }
+}
+
 // Relaxes up to 32 records (one per lane) and feeds the winners to L1.
 // `stage` is this warp's TILE_ARCS * 32 arcs of shared memory.
 template <class Arcs, int K>
@@ -568,15 +601,21 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         // staged and CSR arcs alike and keeps the CSR path's arc order.
         int cur = INT_MAX;
         int4 ta = make_int4(-1, 0, -1, 0), tb = ta;
+        const bool piece = valid && v >= (unsigned)p.n;
         if (valid) {
-            cur = __ldcg(p.dist + v);
+            if (!piece) cur = __ldcg(p.dist + v);
             ta = __ldg(p.tiles + 2 * (size_t)v);
             tb = __ldg(p.tiles + 2 * (size_t)v + 1);
         }
+        if (piece) cur = __ldcg(p.dist + ta.w);  // a piece is as fresh as its owner
+        int npieces = 0, first_piece = 0;
         if (valid && (int)d <= cur) {
             if (ta.x == TILE_CSR) {
                 beg = ta.y;
                 deg = ta.z;
+            } else if (ta.x == TILE_SPLIT) {
+                first_piece = ta.y;
+                npieces = ta.z;
             } else {
                 int2 *st = stage + TILE_ARCS * lane;
                 st[0] = make_int2(ta.x, ta.y);
@@ -587,6 +626,7 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
                 beg = INT_MIN + TILE_ARCS * lane;
             }
         }
+        if (__any_sync(FULL, npieces > 0)) push_pieces(p, q, npieces, first_piece, du);
         __syncwarp();
     } else if (valid) {
         // The three loads are independent: issue them together rather than

@@ -142,6 +142,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
 
     PlainParams p{};
     p.n = n;
+    p.nslots = n;  // the caller's CSR has no split pieces
     p.row = d_row;
     p.arcs = nullptr;
     p.tiles = nullptr;  // the caller's CSR is read in place

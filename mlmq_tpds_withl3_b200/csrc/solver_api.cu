@@ -7,6 +7,7 @@
 #include "sssp_plain.h"
 #include "solver_internal.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -59,6 +60,13 @@ __global__ void tile_kernel(const int *__restrict__ row, const int2 *__restrict_
         tiles[2 * (size_t)v] = make_int4(t[0], t[1], t[2], t[3]);
         tiles[2 * (size_t)v + 1] = make_int4(t[4], t[5], t[6], t[7]);
     }
+}
+
+// Heavy vertices' tiles: {TILE_SPLIT, first piece, pieces, degree}.
+__global__ void patch_tiles_kernel(const int *__restrict__ idx, const int4 *__restrict__ tile,
+                                   int count, int4 *tiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) tiles[2 * (size_t)idx[i]] = tile[i];
 }
 
 __global__ void fill_kernel(int *p, int64_t n, int v) {
@@ -239,12 +247,61 @@ extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const 
         rc = cuda_fail(cudaGetLastError(), "interleave launch");
         if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "interleave");
     }
-    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_tiles, 2 * sizeof(int4) * (size_t)n), "cudaMalloc(tiles)");
+    // Heavy vertices and their pieces, from the row offsets.
+    std::vector<int> heavy;           // vertex ids
+    std::vector<int4> piece_tiles;    // 2 per piece
+    std::vector<int4> heavy_tiles;    // 1 per heavy vertex (first half of its tile)
+    if (!rc) {
+        std::vector<int> row((size_t)n + 1);
+        rc = cuda_fail(cudaMemcpy(row.data(), d_row, sizeof(int) * ((size_t)n + 1),
+                                  cudaMemcpyDeviceToHost), "D2H row");
+        for (int v = 0; !rc && v < n; v++) {
+            const int deg = row[v + 1] - row[v];
+            if (deg <= SPLIT_MIN) continue;
+            const int np = (deg + PIECE_ARCS - 1) / PIECE_ARCS;
+            if ((int64_t)n + g->pieces + np >= INT_MAX) {
+                rc = MLMQ_ERR_RANGE;
+                break;
+            }
+            heavy.push_back(v);
+            heavy_tiles.push_back(make_int4(TILE_SPLIT, n + g->pieces, np, deg));
+            for (int k = 0; k < np; k++) {
+                const int b = row[v] + k * PIECE_ARCS;
+                const int c = std::min(PIECE_ARCS, row[v + 1] - b);
+                piece_tiles.push_back(make_int4(TILE_CSR, b, c, v));
+                piece_tiles.push_back(make_int4(-1, 0, -1, 0));
+            }
+            g->pieces += np;
+        }
+    }
+    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_tiles, 2 * sizeof(int4) * (size_t)g->slots()),
+                            "cudaMalloc(tiles)");
     if (!rc) {
         int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 16);
         tile_kernel<<<blocks, 256>>>(d_row, g->d_arcs, g->d_tiles, n);
         rc = cuda_fail(cudaGetLastError(), "tile launch");
         if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "tiles");
+    }
+    if (!rc && g->pieces > 0) {
+        rc = cuda_fail(cudaMemcpy(g->d_tiles + 2 * (size_t)n, piece_tiles.data(),
+                                  sizeof(int4) * piece_tiles.size(), cudaMemcpyHostToDevice),
+                       "H2D piece tiles");
+        int *d_idx = nullptr;
+        int4 *d_ht = nullptr;
+        if (!rc) rc = cuda_fail(cudaMalloc(&d_idx, sizeof(int) * heavy.size()), "cudaMalloc(heavy)");
+        if (!rc) rc = cuda_fail(cudaMalloc(&d_ht, sizeof(int4) * heavy.size()), "cudaMalloc(heavy tiles)");
+        if (!rc) rc = cuda_fail(cudaMemcpy(d_idx, heavy.data(), sizeof(int) * heavy.size(),
+                                           cudaMemcpyHostToDevice), "H2D heavy");
+        if (!rc) rc = cuda_fail(cudaMemcpy(d_ht, heavy_tiles.data(), sizeof(int4) * heavy.size(),
+                                           cudaMemcpyHostToDevice), "H2D heavy tiles");
+        if (!rc) {
+            const int hn = (int)heavy.size();
+            patch_tiles_kernel<<<(hn + 255) / 256, 256>>>(d_idx, d_ht, hn, g->d_tiles);
+            rc = cuda_fail(cudaGetLastError(), "patch launch");
+            if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "patch tiles");
+        }
+        cudaFree(d_idx);
+        cudaFree(d_ht);
     }
     if (rc) {
         mlmq_graph_free(g);
@@ -284,6 +341,12 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
     return MLMQ_OK;
 }
 
+extern "C" int mlmq_graph_pieces(const mlmq_graph *g, int *pieces) {
+    if (!g || !pieces) return MLMQ_ERR_ARG;
+    *pieces = g->pieces;
+    return MLMQ_OK;
+}
+
 extern "C" int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m) {
     if (!g) return MLMQ_ERR_ARG;
     if (n) *n = g->n;
@@ -320,7 +383,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
     s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
-    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(g->n, g->m);
+    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(g->slots(), g->m);
     s->workers = cfg.warps_per_block;
     int bps = 0;
     rc = cuda_fail(plain_max_blocks_per_sm(s->workers, cfg.relax_unroll, &bps), "occupancy");
@@ -337,7 +400,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_dist, sizeof(int) * (size_t)g->n), "cudaMalloc(dist)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l2, l2_bytes), "cudaMalloc(L2)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3, l3_bytes), "cudaMalloc(L3)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(g->n)), "cudaMalloc(L3 bits)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(g->slots())), "cudaMalloc(L3 bits)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS), "cudaMalloc(ctl)");
     if (!rc) rc = cuda_fail(cudaMallocHost(&s->h_ctl, sizeof(unsigned) * ctl::WORDS), "pinned ctl");
     if (!rc) rc = fill_device(s->d_dist, g->n, INT_MAX, s->stream);
@@ -375,6 +438,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     if (s->dirty && (rc = reset_workspace(s, st))) return rc;
     PlainParams p;
     p.n = s->g->n;
+    p.nslots = s->g->slots();
     p.row = s->g->d_row;
     p.arcs = s->g->d_arcs;
     p.tiles = s->cfg.vertex_tiles ? s->g->d_tiles : nullptr;

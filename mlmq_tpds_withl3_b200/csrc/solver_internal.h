@@ -14,7 +14,9 @@ struct mlmq_graph {
     int *d_row = nullptr;   // n + 1 row offsets (owned when own_row)
     bool own_row = false;
     int2 *d_arcs = nullptr; // m interleaved {dst, weight} (always owned)
-    int4 *d_tiles = nullptr; // 2 per vertex: the vertex tile (mlmq_queue.cuh; always owned)
+    int4 *d_tiles = nullptr; // 2 per vertex and per piece: the vertex tiles (always owned)
+    int pieces = 0;          // virtual vertices n .. n + pieces - 1 (split heavy vertices)
+    int slots() const { return n + pieces; }
 };
 
 struct mlmq_solver {

@@ -37,7 +37,7 @@ struct BatchQuery {
     const int *row;
     const int2 *arcs;
     const int4 *tiles;
-    int n, src;
+    int n, nslots, src;
 };
 struct BatchParams {
     PlainParams base;  // configuration; dist/l2/l3/l3bits/ctlw point at slot 0's arrays
@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_batch_kernel(BatchP
     p.arcs = qy.arcs;
     p.tiles = qy.tiles;
     p.n = qy.n;
+    p.nslots = qy.nslots;
     p.src = qy.src;
     p.dist = bp.base.dist + s * bp.dist_stride;
     p.l2 = bp.base.l2 + s * bp.l2_stride;
@@ -256,7 +257,7 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
                               const int *srcs, int use_graph, void *stream) {
     if (!b || nq < 1 || nq > b->max_q || !graphs || !srcs) return MLMQ_ERR_ARG;
     for (int q = 0; q < nq; q++) {
-        if (!graphs[q] || graphs[q]->n > b->max_n || srcs[q] < 0 || srcs[q] >= graphs[q]->n)
+        if (!graphs[q] || graphs[q]->slots() > b->max_n || srcs[q] < 0 || srcs[q] >= graphs[q]->n)
             return MLMQ_ERR_ARG;
         if (graphs[q]->device != b->device) return MLMQ_ERR_ARG;
     }
@@ -273,6 +274,7 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         qy.arcs = g->d_arcs;
         qy.tiles = b->cfg.vertex_tiles ? g->d_tiles : nullptr;
         qy.n = g->n;
+        qy.nslots = g->slots();
         qy.src = srcs[q];
         b->n_of[q] = g->n;
         key.push_back((long long)(uintptr_t)g);

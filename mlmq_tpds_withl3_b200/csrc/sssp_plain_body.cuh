@@ -211,7 +211,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     const size_t gtid = (size_t)grank * blockDim.x + threadIdx.x;
     const size_t gstride = (size_t)gsize * blockDim.x;
     for (size_t i = gtid; i < (size_t)p.n; i += gstride) p.dist[i] = INT_MAX;
-    for (size_t i = gtid; i < ((size_t)p.n + 31) / 32; i += gstride) p.l3bits[i] = 0u;
+    for (size_t i = gtid; i < ((size_t)p.nslots + 31) / 32; i += gstride) p.l3bits[i] = 0u;
     if (grank == 0) {
         for (int i = threadIdx.x; i < ctl::WORDS; i += blockDim.x)
             if (i != ctl::BAR_COUNT && i != ctl::BAR_GEN) p.ctlw[i] = 0u;

@@ -39,7 +39,7 @@ constexpr int SRV_CTL_STRIDE = 512;  // words per slot control block
 // Words of the slot control block used by the server around a solve (the
 // solve itself uses words below ctl::WORDS).
 constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs, tiles (2 words each),
-                                  // n, src, delta, topup, l1_ahead, bucket_max
+                                  // n, src, delta, topup, l1_ahead, bucket_max, nslots
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_BAR_COUNT = 488;
@@ -60,6 +60,7 @@ struct alignas(64) SlotCommand {
     const int4 *tiles;
     int n;
     int src;
+    int nslots;
     // per-query settings (the server's configuration unless overridden)
     unsigned delta;
     int topup, l1_ahead, bm;
@@ -160,6 +161,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                         c[SRV_CMD + 9] = (unsigned)sp.cmd[s].topup;
                         c[SRV_CMD + 10] = (unsigned)sp.cmd[s].l1_ahead;
                         c[SRV_CMD + 11] = (unsigned)sp.cmd[s].bm;
+                        c[SRV_CMD + 12] = (unsigned)sp.cmd[s].nslots;
                         __threadfence();
                         // publish the sequence number (low 32 bits) to the group
                         st_release(c + SRV_GO, (unsigned)q);
@@ -197,6 +199,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         p.topup = (int)cmd[9];
         p.l1_ahead = (int)cmd[10];
         p.bm = (int)cmd[11];
+        p.nslots = (int)cmd[12];
         p.n = (int)cmd[4];
         p.src = (int)cmd[5];
         p.dist = sp.dist + (size_t)s * sp.max_n;
@@ -425,7 +428,7 @@ extern "C" int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, in
 
 extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int src,
                                       const mlmq_config *knobs, int *h_out, uint64_t *ticket) {
-    if (!sv || !g || !h_out || !ticket || src < 0 || src >= g->n || g->n > sv->max_n)
+    if (!sv || !g || !h_out || !ticket || src < 0 || src >= g->n || g->slots() > sv->max_n)
         return MLMQ_ERR_ARG;
     if (g->device != sv->device) return MLMQ_ERR_ARG;
     const mlmq_config &k = knobs ? *knobs : sv->cfg;
@@ -447,6 +450,7 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     cmd.arcs = g->d_arcs;
     cmd.tiles = sv->cfg.vertex_tiles ? g->d_tiles : nullptr;
     cmd.n = g->n;
+    cmd.nslots = g->slots();
     cmd.src = src;
     cmd.delta = (unsigned)k.delta;
     cmd.topup = k.topup;

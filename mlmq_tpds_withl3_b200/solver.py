@@ -24,6 +24,12 @@ class DeviceGraph:
     def __init__(self, handle, n, m):
         self._h = ctypes.c_void_p(handle)
         self.n, self.m = n, m
+        pc = ctypes.c_int()
+        check(lib.mlmq_graph_pieces(self._h, ctypes.byref(pc)), "mlmq_graph_pieces")
+        # vertex slots a batch or server needs for this graph: n plus the
+        # pieces of its split heavy vertices
+        self.pieces = pc.value
+        self.slots = n + pc.value
 
     @classmethod
     def upload(cls, hg):

@@ -32,7 +32,7 @@ def test_uneven_graphs_in_one_launch():
         for s in (0, g.n - 1):
             queries.append((dg, s))
             refs.append(oracle_lib.sssp_i32(g, s)[0])
-    b = BatchSolver(len(queries), max(g.n for g in graphs))
+    b = BatchSolver(len(queries), max(dg.slots for dg in dgs))
     b.run(queries)
     for q, ref in enumerate(refs):
         assert np.array_equal(b.dist(q), ref), q

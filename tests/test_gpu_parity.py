@@ -104,6 +104,29 @@ def test_live_solvers_with_different_cta_sizes():
         assert np.array_equal(s.solve(7).dist(), ref)
 
 
+def test_split_heavy_vertices_exact():
+    """Vertices of more than 1024 arcs are relaxed as 512-arc pieces taken by
+    different warps; single, batched and tile-less solves stay exact."""
+    from mlmq_tpds_withl3_b200 import BatchSolver
+    g = HostGraph.rmat(16, seed=13)
+    dg = DeviceGraph.upload(g)
+    assert dg.pieces > 0 and dg.slots == g.n + dg.pieces
+    srcs = [0, 1, 2]
+    ref, _ = oracle_lib.sssp_many(g, srcs)
+    s = Solver(dg)
+    flat = Solver(dg, {"vertex_tiles": 0})
+    for k, src in enumerate(srcs):
+        assert np.array_equal(s.solve(src).dist(), ref[k]), src
+        assert np.array_equal(flat.solve(src).dist(), ref[k]), src
+    b = BatchSolver(len(srcs), dg.slots, {"topup": 32})
+    b.run([(dg, x) for x in srcs])
+    for k in range(len(srcs)):
+        assert np.array_equal(b.dist(k), ref[k])
+    # narrow buckets push pieces through L3 as well
+    t = Solver(dg, {"bucket_num": 2, "bucket_max": 1, "delta": 3000, "timeout_ms": 15000})
+    assert np.array_equal(t.solve(0).dist(), ref[0])
+
+
 def test_knn_and_rmat_medium():
     for g in (HostGraph.knn(200000, seed=2), HostGraph.rmat(16, seed=3)):
         s = Solver(DeviceGraph.upload(g))

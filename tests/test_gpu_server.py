@@ -19,7 +19,7 @@ def _graphs():
 def test_served_results_equal_oracle_and_alone():
     hgs = _graphs()
     dgs = [DeviceGraph.upload(g) for g in hgs]
-    sv = Server(slots=12, max_vertices=max(g.n for g in hgs), lifetime_s=120)
+    sv = Server(slots=12, max_vertices=max(dg.slots for dg in dgs), lifetime_s=120)
     sched = poisson_schedule(rate=3000.0, count=80, graphs_n=[g.n for g in hgs], seed=7)
     recs = serve_poisson(sv, dgs, sched, keep=lambda i: True, timeout_s=60)
     sv.close()
