@@ -67,6 +67,10 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--max-queries", type=int, default=4000)
     ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--wide-slots", type=int, default=0,
+                    help="served: wide slots for throughput-bound graphs (0: all slots equal; "
+                         "on the 8-graph mix equal slots measured best)")
+    ap.add_argument("--wide-ctas", type=int, default=54, help="served: CTAs of a wide slot")
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
     ap.add_argument("--side", type=int, default=0,
                     help="c4: grid side instead of 4896 (small cases for profiler captures)")
@@ -506,22 +510,43 @@ def run_served(args):
     tune_report = None
     cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2)
     knobs = None
+    layout = None
+    grid_max = 3 * 148  # CTAs of 8+1 warps that fit a B200 (the server checks)
+    if args.wide_slots > 0:
+        small = (grid_max - args.wide_slots * args.wide_ctas) // 6
+        layout = [6] * small + [args.wide_ctas] * args.wide_slots
     if not args.no_tune:
         # Each resident graph gets the per-query settings (delta, topup,
         # run-ahead bound) that were fastest on a batched launch of 64 of its
-        # own queries; the server passes them with every query on that graph.
+        # own queries in small slots, and is sent to a wide slot when 8 of its
+        # queries in wide slots give more queries/s than that (a
+        # throughput-bound query gains nothing from sharing the GPU in small
+        # pieces).  The server passes the settings with every query.
         from mlmq_tpds_withl3_b200 import autotune
         cands = [{"delta": d, "topup": t} for d in (50000, 100000, 200000) for t in (16, 32)]
         cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0}]
         knobs, tune_report = [], {}
+        base = {"warps_per_block": 8, "relax_unroll": 2}
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
-            kc, rep = autotune.tune_batch(qs, dg.slots, candidates=cands,
-                                          base={"warps_per_block": 8, "relax_unroll": 2})
+            kc, rep = autotune.tune_batch(qs, dg.slots, candidates=cands, base=base)
+            entry = dict(rep["config"])
+            if layout is not None:
+                qps_small = len(qs) / rep["seconds"]
+                kw, repw = autotune.tune_batch(
+                    qs[:8], dg.slots, candidates=cands,
+                    base={**base, "work_blocks": 8 * args.wide_ctas})
+                qps_wide = 8 / repw["seconds"]
+                entry["qps_small_slots"] = qps_small
+                entry["qps_wide_slots"] = qps_wide
+                if qps_wide > qps_small:
+                    kc = default_config(**{**base, **repw["config"], "work_blocks": args.wide_ctas})
+                    entry = {**repw["config"], "work_blocks": args.wide_ctas,
+                             "qps_small_slots": qps_small, "qps_wide_slots": qps_wide}
             knobs.append(kc)
-            tune_report[names[i]] = rep["config"]
-    sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900)
+            tune_report[names[i]] = entry
+    sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900, layout=layout)
     pool = PinnedPool(sv.slots, max_n)
     rates = [float(r) for r in args.rates.split(",")]
     sweep = []
@@ -581,6 +606,8 @@ def run_served(args):
                                "arrivals, graph and source uniform per query",
                    "graphs": {k: {"n": hgs[k].n, "m": hgs[k].m} for k in names},
                    "slots": sv.slots, "grid": sv.grid, "delta": cfg.delta,
+                   "slot_ctas": sorted(set(sv.layout)) if layout else None,
+                   "wide_slots": args.wide_slots if layout else 0,
                    "warps_per_block": cfg.warps_per_block, "relax_unroll": cfg.relax_unroll,
                    "l1_ahead": cfg.l1_ahead, "rates": rates},
         "sweep": sweep,

@@ -289,14 +289,26 @@ void mlmq_batch_destroy(mlmq_batch *b);
 typedef struct mlmq_server mlmq_server;
 int mlmq_server_create(int slots, int max_vertices, const mlmq_config *cfg, int lifetime_ms,
                        mlmq_server **out);
+/* As mlmq_server_create with slots of different sizes: slot s gets
+ * slot_ctas[s] CTAs (their sum must fit the GPU's co-resident grid).  A
+ * query asks for a slot size with mlmq_server_submit_cfg's knobs->work_blocks
+ * and gets the smallest free slot of at least that many CTAs: small slots
+ * suit latency-bound queries (many run side by side), wide ones
+ * throughput-bound queries.  MLMQ_ERR_NOMEM if the slots do not all fit in
+ * device memory. */
+int mlmq_server_create_layout(int slots, const int *slot_ctas, int max_vertices,
+                              const mlmq_config *cfg, int lifetime_ms, mlmq_server **out);
+/* CTAs of each slot (up to `max` entries); *count = number of slots. */
+int mlmq_server_layout(const mlmq_server *sv, int *slot_ctas, int max, int *count);
 int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block);
 /* Non-blocking.  MLMQ_ERR_BUSY when every slot is taken; h_out (n ints) must
  * stay valid until the ticket is reported by mlmq_server_poll. */
 int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
                        uint64_t *ticket);
 /* As mlmq_server_submit, with this query's delta, topup, l1_ahead and
- * bucket_max taken from *knobs (the other fields are fixed per server and
- * ignored; NULL = the server's configuration), so queries on graphs of
+ * bucket_max taken from *knobs, and knobs->work_blocks = the smallest slot
+ * (CTAs) it may run in (the other fields are fixed per server and ignored;
+ * NULL = the server's configuration, any slot), so queries on graphs of
  * different shapes can each run their own tuned settings in one server. */
 int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int src,
                            const mlmq_config *knobs, int *h_out, uint64_t *ticket);

@@ -138,6 +138,9 @@ _sig("mlmq_batch_destroy", None, c_vp)
 # continuous-batching server
 _sig("mlmq_server_create", c_int, c_int, c_int, ctypes.POINTER(Config), c_int,
      ctypes.POINTER(c_vp))
+_sig("mlmq_server_create_layout", c_int, c_int, ctypes.POINTER(c_int), c_int, ctypes.POINTER(Config),
+     c_int, ctypes.POINTER(c_vp))
+_sig("mlmq_server_layout", c_int, c_vp, ctypes.POINTER(c_int), c_int, ctypes.POINTER(c_int))
 _sig("mlmq_server_info", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
      ctypes.POINTER(c_int))
 _sig("mlmq_server_submit", c_int, c_vp, c_vp, c_int, c_vp, ctypes.POINTER(c_u64))

@@ -83,6 +83,8 @@ struct ServerParams {
     unsigned *l3bits;             // slots * bits_words
     size_t bits_words;
     unsigned *ctl;                // slots * SRV_CTL_STRIDE
+    const int *cta_slot;          // [grid] slot of each CTA
+    const int *slot_first;        // [slots + 1] first CTA of each slot
     int slots, max_n;
     unsigned long long lifetime_ns;
 };
@@ -119,11 +121,12 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
 // budget of PLAIN_MAX_THREADS threads.
 template <int K>
 __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(ServerParams sp) {
-    const unsigned g = gridDim.x;
-    const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * (unsigned)sp.slots) / g);
-    const unsigned lo = (unsigned)(((unsigned long long)s * g + sp.slots - 1) / (unsigned)sp.slots);
-    const unsigned hi =
-        (unsigned)(((unsigned long long)(s + 1) * g + sp.slots - 1) / (unsigned)sp.slots);
+    // Slot s is the CTA group [slot_first[s], slot_first[s + 1]); slots may
+    // differ in size (small ones for latency-bound queries, wide ones for
+    // throughput-bound queries).
+    const unsigned s = (unsigned)sp.cta_slot[blockIdx.x];
+    const unsigned lo = (unsigned)sp.slot_first[s];
+    const unsigned hi = (unsigned)sp.slot_first[s + 1];
     const unsigned grank = blockIdx.x - lo, gsize = hi - lo;
     unsigned *c = sp.ctl + (size_t)s * SRV_CTL_STRIDE;
     const unsigned long long end = globaltimer() + sp.lifetime_ns;
@@ -265,6 +268,8 @@ struct mlmq_server {
     unsigned *d_l3bits = nullptr;
     size_t bits_words = 0;
     unsigned *d_ctl = nullptr;
+    int *d_cta_slot = nullptr, *d_slot_first = nullptr;
+    std::vector<int> slot_ctas;   // CTAs of each slot
     SlotCommand *h_cmd = nullptr;
     SlotCompletion *h_done = nullptr;
     unsigned *h_shutdown = nullptr;
@@ -288,9 +293,17 @@ struct mlmq_server {
     std::deque<std::pair<unsigned long long, int>> finished;  // (ticket, status)
 };
 
-extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config *cfg_in,
-                                  int lifetime_ms, mlmq_server **out) {
+namespace {
+
+// `layout` (CTAs per slot, `slots` entries) or null for an even split of the
+// largest co-resident grid into at most `slots` slots (fewer when device
+// memory runs short).
+int server_create(int slots, const int *layout, int max_vertices, const mlmq_config *cfg_in,
+                  int lifetime_ms, mlmq_server **out) {
     if (!out || slots < 1 || max_vertices < 1 || lifetime_ms < 1) return MLMQ_ERR_ARG;
+    if (layout)
+        for (int s = 0; s < slots; s++)
+            if (layout[s] < 1) return MLMQ_ERR_ARG;
     mlmq_config cfg;
     int rc = MLMQ_OK;
     if (cfg_in) cfg = *cfg_in;
@@ -321,7 +334,7 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         const size_t reserve = (size_t)2 << 30;
         const size_t fit = free_b > reserve ? (free_b - reserve) / per_slot : 0;
         sv->slots = (int)std::min<size_t>((size_t)slots, fit);
-        if (sv->slots < 1) rc = MLMQ_ERR_NOMEM;
+        if (sv->slots < 1 || (layout && sv->slots < slots)) rc = MLMQ_ERR_NOMEM;
     }
     int bps = 0;
     const int threads = 32 * (sv->workers + 1);
@@ -331,11 +344,37 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
                                                  (int)plain_smem_limit()), "server smem");
     if (!rc) rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem),
                             "server occupancy");
-    if (!rc) {
+    if (!rc && layout) {
+        long long total = 0;
+        for (int s = 0; s < slots; s++) total += layout[s];
+        if (total > (long long)bps * sms) {
+            std::fprintf(stderr, "mlmq_server_create_layout: %lld CTAs requested, %d fit\n", total,
+                         bps * sms);
+            rc = MLMQ_ERR_RANGE;
+        } else {
+            sv->grid = (int)total;
+            sv->slot_ctas.assign(layout, layout + slots);
+        }
+    } else if (!rc) {
         sv->grid = cfg.work_blocks > 0 ? std::min(cfg.work_blocks, bps * sms) : bps * sms;
         sv->slots = std::min(sv->slots, sv->grid);
+        const long long g = sv->grid, n = sv->slots;
+        for (long long s = 0; s < n; s++)
+            sv->slot_ctas.push_back((int)(((s + 1) * g + n - 1) / n - (s * g + n - 1) / n));
     }
     const size_t ns = (size_t)sv->slots;
+    std::vector<int> cta_slot, slot_first(1, 0);
+    for (int s = 0; s < (int)sv->slot_ctas.size(); s++) {
+        for (int c = 0; c < sv->slot_ctas[s]; c++) cta_slot.push_back(s);
+        slot_first.push_back(slot_first.back() + sv->slot_ctas[s]);
+    }
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_cta_slot, sizeof(int) * cta_slot.size()), "server CTA map");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_slot_first, sizeof(int) * slot_first.size()), "server slots");
+    if (!rc) rc = cuda_fail(cudaMemcpy(sv->d_cta_slot, cta_slot.data(), sizeof(int) * cta_slot.size(),
+                                       cudaMemcpyHostToDevice), "H2D CTA map");
+    if (!rc) rc = cuda_fail(cudaMemcpy(sv->d_slot_first, slot_first.data(),
+                                       sizeof(int) * slot_first.size(), cudaMemcpyHostToDevice),
+                            "H2D slots");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_dist, sizeof(int) * ns * (size_t)max_vertices), "server dist");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l2, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log)), "server L2");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3, 8 * (ns << sv->l3_log)), "server L3");
@@ -390,6 +429,8 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
         sp.l3bits = sv->d_l3bits;
         sp.bits_words = sv->bits_words;
         sp.ctl = sv->d_ctl;
+        sp.cta_slot = sv->d_cta_slot;
+        sp.slot_first = sv->d_slot_first;
         sp.slots = sv->slots;
         sp.max_n = max_vertices;
         sp.lifetime_ns = (unsigned long long)lifetime_ms * 1000000ull;
@@ -418,6 +459,28 @@ extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config
     return MLMQ_OK;
 }
 
+}  // namespace
+
+extern "C" int mlmq_server_create(int slots, int max_vertices, const mlmq_config *cfg,
+                                  int lifetime_ms, mlmq_server **out) {
+    return server_create(slots, nullptr, max_vertices, cfg, lifetime_ms, out);
+}
+
+extern "C" int mlmq_server_create_layout(int slots, const int *slot_ctas, int max_vertices,
+                                         const mlmq_config *cfg, int lifetime_ms,
+                                         mlmq_server **out) {
+    if (!slot_ctas) return MLMQ_ERR_ARG;
+    return server_create(slots, slot_ctas, max_vertices, cfg, lifetime_ms, out);
+}
+
+extern "C" int mlmq_server_layout(const mlmq_server *sv, int *slot_ctas, int max, int *count) {
+    if (!sv || !count || (max > 0 && !slot_ctas)) return MLMQ_ERR_ARG;
+    const int n = (int)sv->slot_ctas.size();
+    for (int s = 0; s < n && s < max; s++) slot_ctas[s] = sv->slot_ctas[s];
+    *count = n;
+    return MLMQ_OK;
+}
+
 extern "C" int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block) {
     if (!sv) return MLMQ_ERR_ARG;
     if (slots) *slots = sv->slots;
@@ -435,14 +498,16 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     if (k.delta < 1 || k.topup < 0 || k.topup > 32 || k.l1_ahead < 0 || k.bucket_max < 1 ||
         k.bucket_max > sv->cfg.bucket_num)
         return MLMQ_ERR_ARG;
+    // The smallest free slot with at least the CTAs the query asks for
+    // (knobs->work_blocks; 0 or no knobs: any).
+    const int want = knobs ? knobs->work_blocks : 0;
     std::lock_guard<std::mutex> lk(sv->mu);
     if (!sv->running) return MLMQ_ERR_STATE;
     int free_slot = -1;
     for (int s = 0; s < sv->slots; s++)
-        if (!sv->st[s].busy) {
+        if (!sv->st[s].busy && sv->slot_ctas[s] >= want &&
+            (free_slot < 0 || sv->slot_ctas[s] < sv->slot_ctas[free_slot]))
             free_slot = s;
-            break;
-        }
     if (free_slot < 0) return MLMQ_ERR_BUSY;
     auto &sl = sv->st[free_slot];
     SlotCommand &cmd = sv->h_cmd[free_slot];
@@ -544,6 +609,8 @@ extern "C" void mlmq_server_destroy(mlmq_server *sv) {
     cudaFree(sv->d_l3);
     cudaFree(sv->d_l3bits);
     cudaFree(sv->d_ctl);
+    cudaFree(sv->d_cta_slot);
+    cudaFree(sv->d_slot_first);
     if (sv->h_cmd) cudaFreeHost(sv->h_cmd);
     if (sv->h_done) cudaFreeHost(sv->h_done);
     if (sv->h_shutdown) cudaFreeHost(sv->h_shutdown);

@@ -21,17 +21,33 @@ from ._lib import MLMQ_ERR_BUSY, check, lib
 
 
 class Server:
-    def __init__(self, slots, max_vertices, cfg=None, lifetime_s=600.0):
+    """`slots` query slots of equal size, or `layout` = CTAs of each slot
+    (small slots for latency-bound queries, wide ones for throughput-bound
+    queries; a query's knobs.work_blocks asks for a slot of at least that
+    many CTAs)."""
+
+    def __init__(self, slots, max_vertices, cfg=None, lifetime_s=600.0, layout=None):
         if cfg is None or isinstance(cfg, dict):
             cfg = _lib.default_config(**{"warps_per_block": 8, **(cfg or {})})
         self.cfg = cfg
         h = ctypes.c_void_p()
-        check(lib.mlmq_server_create(slots, max_vertices, ctypes.byref(cfg),
-                                     int(lifetime_s * 1000), ctypes.byref(h)), "mlmq_server_create")
+        if layout is not None:
+            arr = (ctypes.c_int * len(layout))(*layout)
+            check(lib.mlmq_server_create_layout(len(layout), arr, max_vertices, ctypes.byref(cfg),
+                                                int(lifetime_s * 1000), ctypes.byref(h)),
+                  "mlmq_server_create_layout")
+        else:
+            check(lib.mlmq_server_create(slots, max_vertices, ctypes.byref(cfg),
+                                         int(lifetime_s * 1000), ctypes.byref(h)),
+                  "mlmq_server_create")
         self._h = h
         s, g, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(lib.mlmq_server_info(h, ctypes.byref(s), ctypes.byref(g), ctypes.byref(b)))
         self.slots, self.grid, self.block = s.value, g.value, b.value
+        ctas = (ctypes.c_int * self.slots)()
+        cnt = ctypes.c_int()
+        check(lib.mlmq_server_layout(h, ctas, self.slots, ctypes.byref(cnt)))
+        self.layout = list(ctas[:cnt.value])
         self.max_vertices = max_vertices
         self._tk = (ctypes.c_uint64 * 256)()
         self._st = (ctypes.c_int * 256)()
@@ -111,20 +127,36 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
         now = time.perf_counter() - t0
         if now > timeout_s:
             raise TimeoutError("serving did not finish in time")
-        # admit every arrived query while a slot and a buffer are free
-        while pending and schedule[pending[0]][0] <= now:
+        # Admit arrived queries in arrival order while slots and buffers are
+        # free; a query whose slot size is all taken is passed over (it keeps
+        # its place) so that it does not hold back queries that fit.
+        # A slot class (the CTAs a query asks for) found full is not tried
+        # again in this pass; a query that takes any slot finding none ends it.
+        skipped = []
+        full = set()
+        while pending and schedule[pending[0]][0] <= now and len(skipped) < 256:
             i = pending[0]
+            _, gi, src = schedule[i]
+            kn = knobs[gi] if knobs is not None else None
+            cls = kn.work_blocks if kn is not None else 0
+            pending.popleft()
+            if cls in full:
+                skipped.append(i)
+                continue
             buf = pool.get()
             if buf is None:
+                skipped.append(i)
                 break
-            _, gi, src = schedule[i]
-            tk = server.submit(dgraphs[gi], src, buf,
-                               knobs[gi] if knobs is not None else None)
+            tk = server.submit(dgraphs[gi], src, buf, kn)
             if tk is None:
                 pool.put(buf)
-                break
-            pending.popleft()
+                skipped.append(i)
+                full.add(cls)
+                if cls == 0:
+                    break
+                continue
             inflight[tk] = (i, buf, now)
+        pending.extendleft(reversed(skipped))
         for tk, status in server.poll():
             i, buf, start = inflight.pop(tk)
             arr, gi, src = schedule[i]

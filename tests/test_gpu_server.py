@@ -65,6 +65,36 @@ def test_per_query_settings_give_the_same_result():
         assert np.array_equal(b.numpy(), ref)
 
 
+def test_slot_layout_and_slot_choice():
+    """Slots of different sizes: a query asking for 6 CTAs gets the wide slot
+    and waits while it is taken; results stay exact."""
+    from mlmq_tpds_withl3_b200 import default_config
+    import torch
+    import time
+    g = HostGraph.grid(150, 150, seed=47)
+    dg = DeviceGraph.upload(g)
+    sv = Server(slots=0, max_vertices=dg.slots, layout=[1, 2, 6], lifetime_s=60)
+    assert sv.layout == [1, 2, 6] and sv.grid == 9
+    wide = default_config(work_blocks=6)
+    bufs = [torch.empty(g.n, dtype=torch.int32, pin_memory=True) for _ in range(4)]
+    t_wide = sv.submit(dg, 3, bufs[0], wide)
+    assert t_wide is not None
+    assert sv.submit(dg, 4, bufs[1], wide) is None  # the only wide slot is taken
+    t_a = sv.submit(dg, 5, bufs[2])                 # smallest free slot
+    t_b = sv.submit(dg, 6, bufs[3])
+    assert t_a is not None and t_b is not None
+    done = {}
+    t0 = time.time()
+    while len(done) < 3 and time.time() - t0 < 30:
+        for tk, st in sv.poll():
+            done[tk] = st
+    sv.close()
+    assert done == {t_wide: 0, t_a: 0, t_b: 0}
+    for src, b in ((3, bufs[0]), (5, bufs[2]), (6, bufs[3])):
+        ref, _ = oracle_lib.sssp_i32(g, src)
+        assert np.array_equal(b.numpy(), ref), src
+
+
 def test_server_busy_and_stop():
     g = HostGraph.grid(64, 64, seed=45)
     dg = DeviceGraph.upload(g)
