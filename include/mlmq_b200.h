@@ -101,6 +101,18 @@ typedef struct mlmq_config {
                             its L1 fills the rest of the warp from L2 in the
                             same iteration (default 0 = off: it lengthens a
                             single solve's critical path; batches use it) */
+    int bucket_sync;     /* 1: the bucket window moves on only when no record
+                            taken from the queues is still being worked on
+                            (bulk-synchronous buckets): fewer redundant
+                            relaxations where buckets are wide and few
+                            (power-law graphs), slower where they are many
+                            (grids); default 0 */
+    int defer_degree;    /* >0: a vertex of at least this many arcs is relaxed
+                            one bucket late (a record for it re-enters at
+                            distance + delta), by then at its final distance,
+                            so hubs of power-law graphs are relaxed about
+                            once; needs vertex tiles and vertex slots
+                            n + pieces + n in batches and servers; default 0 */
     int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
                             32-byte tile (up to 4 arcs inline, else its CSR
                             range); 0: row offsets, then arcs */
@@ -305,8 +317,8 @@ int mlmq_server_info(const mlmq_server *sv, int *slots, int *grid, int *block);
  * stay valid until the ticket is reported by mlmq_server_poll. */
 int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src, int *h_out,
                        uint64_t *ticket);
-/* As mlmq_server_submit, with this query's delta, topup, l1_ahead and
- * bucket_max taken from *knobs, and knobs->work_blocks = the smallest slot
+/* As mlmq_server_submit, with this query's delta, topup, l1_ahead,
+ * bucket_max and bucket_sync taken from *knobs, and knobs->work_blocks = the smallest slot
  * (CTAs) it may run in (the other fields are fixed per server and ignored;
  * NULL = the server's configuration, any slot), so queries on graphs of
  * different shapes can each run their own tuned settings in one server. */

@@ -56,6 +56,7 @@ namespace mlmq {
 struct PlainParams {
     int n;
     int nslots;  // n + split-vertex pieces (ids n .. nslots-1 are pieces)
+    int nids;    // nslots, + n when deferral is on (ids nslots + v: v's deferred record)
     const int *__restrict__ row;
     const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
     const int4 *__restrict__ tiles; // 2 per vertex, or null: read row offsets instead
@@ -71,6 +72,8 @@ struct PlainParams {
     int l1_keep;   // records kept at the L1 front when it spills (0: spill all)
     int l1_ahead;  // buckets past `first` a winner may be to stay in L1 (0: no limit)
     int topup;     // fewer than this many L1 records: fill the warp from L2 too
+    int bucket_sync;  // 1: `first` advances only when no taken record is still in flight
+    int defer_deg;    // >0: vertices of at least this degree are relaxed one bucket late
     int precheck;  // read dist[dst] before the atomicMin
     unsigned delta;
     int l2_log, l3_log;
@@ -444,9 +447,17 @@ __device__ __forceinline__ int l3_rebucket(const PlainParams &p, WarpQ &q, volat
         st_relaxed64(l3_slot(p, s), SENT);
         atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
         __threadfence();
-        // A piece has no distance of its own: its owner's stands for it.
-        const unsigned dv = v < (unsigned)p.n ? v : (unsigned)__ldg(p.tiles + 2 * (size_t)v).w;
-        cur = min((unsigned)__ldcg(p.dist + dv), rec_d(r));
+        // A piece has no distance of its own: its owner's stands for it; a
+        // deferred record stands for its vertex's distance + delta.
+        unsigned dv = v, add = 0u;
+        if (v >= (unsigned)p.nslots) {
+            dv = v - (unsigned)p.nslots;
+            add = p.delta;
+        } else if (v >= (unsigned)p.n) {
+            dv = (unsigned)__ldg(p.tiles + 2 * (size_t)v).w;
+        }
+        const unsigned long long now = (unsigned long long)(unsigned)__ldcg(p.dist + dv) + add;
+        cur = (unsigned)min(now, (unsigned long long)rec_d(r));
     }
     if (take > 0 && lane == 0) atomicAdd(p.ctlw + ctl::L3_CONSUMED, (unsigned)take);
     q.l3_lo += (unsigned)take;
@@ -591,7 +602,13 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
     int beg = 0, deg = 0;
     // Records are relaxed with their own distance: it is the length of a real
     // path, and with the fire-and-forget distance updates the update that
-    // made the record may not be visible here yet.
+    // made the record may not be visible here yet.  A deferred record (id
+    // nslots + v) carries v's distance + delta.
+    const bool deferred = valid && v >= (unsigned)p.nslots;
+    if (deferred) {
+        v -= (unsigned)p.nslots;
+        d -= p.delta;
+    }
     const unsigned du = d;
     if (p.tiles) {
         // Vertex tile: the distance (stale check) and the 32-byte tile are
@@ -609,7 +626,15 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         }
         if (piece) cur = __ldcg(p.dist + ta.w);  // a piece is as fresh as its owner
         int npieces = 0, first_piece = 0;
-        if (valid && (int)d <= cur) {
+        bool defer_now = false;
+        if (valid && (int)d <= cur && !deferred && !piece && p.defer_deg > 0) {
+            // A vertex of high degree waits one bucket: by the time the window
+            // reaches d + delta every improvement of its distance has arrived,
+            // so its (many) arcs are relaxed once, with the final distance.
+            const int vdeg = ta.x == TILE_CSR ? ta.z : (ta.x == TILE_SPLIT ? ta.w : 0);
+            defer_now = vdeg >= p.defer_deg && d < (unsigned)INT_MAX - p.delta;
+        }
+        if (valid && (int)d <= cur && !defer_now) {
             if (ta.x == TILE_CSR) {
                 beg = ta.y;
                 deg = ta.z;
@@ -627,6 +652,8 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
             }
         }
         if (__any_sync(FULL, npieces > 0)) push_pieces(p, q, npieces, first_piece, du);
+        if (__any_sync(FULL, defer_now))
+            push32(p, q, defer_now, (unsigned)p.nslots + v, d + p.delta);
         __syncwarp();
     } else if (valid) {
         // The three loads are independent: issue them together rather than

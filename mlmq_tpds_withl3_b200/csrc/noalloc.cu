@@ -143,6 +143,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     PlainParams p{};
     p.n = n;
     p.nslots = n;  // the caller's CSR has no split pieces
+    p.nids = n;
     p.row = d_row;
     p.arcs = nullptr;
     p.tiles = nullptr;  // the caller's CSR is read in place
@@ -164,6 +165,8 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.l1_keep = cfg.l1_keep;
     p.l1_ahead = cfg.l1_ahead;
     p.topup = cfg.topup;
+    p.bucket_sync = cfg.bucket_sync;
+    p.defer_deg = 0;  // deferral needs vertex tiles
     p.precheck = cfg.relax_precheck;
     p.delta = (unsigned)cfg.delta;
     p.l2_log = NA_L2_LOG;

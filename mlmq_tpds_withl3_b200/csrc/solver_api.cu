@@ -134,6 +134,8 @@ int validate_config(const mlmq_config &c) {
     if (c.vertex_tiles != 0 && c.vertex_tiles != 1) return MLMQ_ERR_ARG;
     if (c.l1_ahead < 0) return MLMQ_ERR_ARG;
     if (c.topup < 0 || c.topup > 32) return MLMQ_ERR_ARG;
+    if (c.bucket_sync != 0 && c.bucket_sync != 1) return MLMQ_ERR_ARG;
+    if (c.defer_degree < 0) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -149,15 +151,19 @@ int device_sm_count(int *sms) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    cudaDeviceProp prop;
-    e = cudaGetDeviceProperties(&prop, dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
-    if (prop.major < 10) {
+    // Two attribute queries (cudaGetDeviceProperties would fill in every
+    // property, a cost paid on every solver creation).
+    int major = 0, minor = 0, count = 0;
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    if (major < 10) {
         std::fprintf(stderr, "mlmq_b200: device %d is sm_%d%d; this library is built for sm_100a\n",
-                     dev, prop.major, prop.minor);
+                     dev, major, minor);
         return MLMQ_ERR_NODEV;
     }
-    *sms = prop.multiProcessorCount;
+    *sms = count;
     return MLMQ_OK;
 }
 
@@ -227,8 +233,12 @@ extern "C" int mlmq_config_default(mlmq_config *cfg) {
 
 // ---- device graphs -----------------------------------------------------------
 
-extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
-                                      const int *d_w, mlmq_graph **out) {
+namespace {
+
+// `h_row`: the same row offsets in host memory when the caller has them
+// (saves copying them back to find the heavy vertices), else null.
+int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int *d_w,
+                const int *h_row, mlmq_graph **out) {
     if (!out || n <= 0 || m < 0 || m >= INT_MAX || !d_row || (m > 0 && (!d_col || !d_w)))
         return MLMQ_ERR_ARG;
     auto *g = new (std::nothrow) mlmq_graph;
@@ -251,10 +261,15 @@ extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const 
     std::vector<int> heavy;           // vertex ids
     std::vector<int4> piece_tiles;    // 2 per piece
     std::vector<int4> heavy_tiles;    // 1 per heavy vertex (first half of its tile)
-    if (!rc) {
-        std::vector<int> row((size_t)n + 1);
-        rc = cuda_fail(cudaMemcpy(row.data(), d_row, sizeof(int) * ((size_t)n + 1),
+    std::vector<int> row_copy;
+    const int *row = h_row;
+    if (!rc && !row) {
+        row_copy.resize((size_t)n + 1);
+        rc = cuda_fail(cudaMemcpy(row_copy.data(), d_row, sizeof(int) * ((size_t)n + 1),
                                   cudaMemcpyDeviceToHost), "D2H row");
+        row = row_copy.data();
+    }
+    if (!rc) {
         for (int v = 0; !rc && v < n; v++) {
             const int deg = row[v + 1] - row[v];
             if (deg <= SPLIT_MIN) continue;
@@ -311,6 +326,13 @@ extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const 
     return MLMQ_OK;
 }
 
+}  // namespace
+
+extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
+                                      const int *d_w, mlmq_graph **out) {
+    return wrap_device(n, m, d_row, d_col, d_w, nullptr, out);
+}
+
 extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
                                  mlmq_graph **out) {
     if (!out || n <= 0 || m < 0 || m >= INT_MAX || !row || (m > 0 && (!col || !w)))
@@ -329,7 +351,7 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
         rc = cuda_fail(cudaMemcpy(d_w, w, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
                        "H2D w");
     mlmq_graph *g = nullptr;
-    if (!rc) rc = mlmq_graph_wrap_device(n, m, d_row, d_col, d_w, &g);
+    if (!rc) rc = wrap_device(n, m, d_row, d_col, d_w, row, &g);
     if (d_col) cudaFree(d_col);
     if (d_w) cudaFree(d_w);
     if (rc) {
@@ -383,7 +405,8 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
     s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
-    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(g->slots(), g->m);
+    s->nids = g->slots() + (cfg.defer_degree ? g->n : 0);
+    s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(s->nids, g->m);
     s->workers = cfg.warps_per_block;
     int bps = 0;
     rc = cuda_fail(plain_max_blocks_per_sm(s->workers, cfg.relax_unroll, &bps), "occupancy");
@@ -400,7 +423,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_dist, sizeof(int) * (size_t)g->n), "cudaMalloc(dist)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l2, l2_bytes), "cudaMalloc(L2)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3, l3_bytes), "cudaMalloc(L3)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(g->slots())), "cudaMalloc(L3 bits)");
+    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(s->nids)), "cudaMalloc(L3 bits)");
     if (!rc) rc = cuda_fail(cudaMalloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS), "cudaMalloc(ctl)");
     if (!rc) rc = cuda_fail(cudaMallocHost(&s->h_ctl, sizeof(unsigned) * ctl::WORDS), "pinned ctl");
     if (!rc) rc = fill_device(s->d_dist, g->n, INT_MAX, s->stream);
@@ -439,6 +462,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     PlainParams p;
     p.n = s->g->n;
     p.nslots = s->g->slots();
+    p.nids = s->nids;
     p.row = s->g->d_row;
     p.arcs = s->g->d_arcs;
     p.tiles = s->cfg.vertex_tiles ? s->g->d_tiles : nullptr;
@@ -460,6 +484,8 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.l1_keep = s->cfg.l1_keep;
     p.l1_ahead = s->cfg.l1_ahead;
     p.topup = s->cfg.topup;
+    p.bucket_sync = s->cfg.bucket_sync;
+    p.defer_deg = s->cfg.defer_degree;
     p.precheck = s->cfg.relax_precheck;
     p.delta = (unsigned)s->cfg.delta;
     p.l2_log = s->l2_log;

@@ -25,6 +25,7 @@ struct mlmq_solver {
     int device = 0;
     int grid = 0, workers = 0;
     int l2_log = 0, l3_log = 0;
+    int nids = 0;               // queue ids: vertex slots, + n with deferral
     int *d_dist = nullptr;
     unsigned long long *d_l2 = nullptr;
     unsigned long long *d_l3 = nullptr;

@@ -61,11 +61,16 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
         if (controller && !ex) {
             unsigned sum = lane < rings ? res : 0u;
             unsigned wait = lane < p.nb ? res - con : 0u;
+            unsigned taken = lane < rings ? con : 0u;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 sum += __shfl_xor_sync(FULL, sum, o);
                 wait += __shfl_xor_sync(FULL, wait, o);
+                taken += __shfl_xor_sync(FULL, taken, o);
             }
+            // Records taken from L2/L3 whose work is not finished (credit was
+            // read first, so this can only overstate).
+            const unsigned in_flight = taken + l3k - credit;
             if (sum + l3r == credit) {
                 if (lane == 0) {
                     atomicOr(p.ctlw + ctl::STATUS, ST_DONE);
@@ -84,7 +89,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
             } else {
                 // Urgent records (below the window) still to be read.
                 const unsigned urgent = __shfl_sync(FULL, res - con, p.nb);
-                if (wait != 0 && urgent == 0) {
+                if (wait != 0 && urgent == 0 && (!p.bucket_sync || in_flight == 0)) {
                     // Move `first` towards the first non-empty bucket of the
                     // window, one bucket per step (as the reference's readers
                     // do): a bucket whose records were all taken may still be
@@ -96,7 +101,10 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
                     const unsigned cb = __shfl_sync(FULL, con, b);
                     const unsigned ne = __ballot_sync(FULL, lane < p.nb && rb != cb);
                     const int i0 = ne ? __ffs(ne) - 1 : 0;
-                    if (i0 > 0 && lane == 0) atomicMax(p.ctlw + ctl::FIRST, first + 1u);
+                    // With bucket sync nothing is in flight, so the window
+                    // may jump straight to the first non-empty bucket.
+                    const unsigned step = p.bucket_sync ? (unsigned)i0 : 1u;
+                    if (i0 > 0 && lane == 0) atomicMax(p.ctlw + ctl::FIRST, first + step);
                 }
                 // Release bucket pressure once the ring has drained.
                 if (lane < p.nb && ((pres >> lane) & 1u) && res - con < cap8)
@@ -211,7 +219,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     const size_t gtid = (size_t)grank * blockDim.x + threadIdx.x;
     const size_t gstride = (size_t)gsize * blockDim.x;
     for (size_t i = gtid; i < (size_t)p.n; i += gstride) p.dist[i] = INT_MAX;
-    for (size_t i = gtid; i < ((size_t)p.nslots + 31) / 32; i += gstride) p.l3bits[i] = 0u;
+    for (size_t i = gtid; i < ((size_t)p.nids + 31) / 32; i += gstride) p.l3bits[i] = 0u;
     if (grank == 0) {
         for (int i = threadIdx.x; i < ctl::WORDS; i += blockDim.x)
             if (i != ctl::BAR_COUNT && i != ctl::BAR_GEN) p.ctlw[i] = 0u;

@@ -50,8 +50,12 @@ def c2(points=6_300_000, nsrc=5):
 
 
 def c3(scale=22, nsrc=5):
+    """Sources are drawn among the largest component's vertices with
+    out-degree > 0 (a directed R-MAT vertex without out-arcs reaches only
+    itself)."""
     g = HostGraph.rmat(scale, 16, 0.57, 0.19, 0.19, wmin=1, wmax=1 << 20, seed=SEED)
-    return g, seeded_sources(g, nsrc)
+    comp = largest_component_vertices(g)
+    return g, seeded_sources(g, nsrc, pool=comp[np.diff(g.row)[comp] > 0])
 
 
 def c4(side=4896, nsrc=64):

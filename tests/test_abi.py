@@ -51,7 +51,7 @@ def test_cxx_dropin_symbols_exported():
 
 def test_struct_layouts():
     assert ctypes.sizeof(_lib.GraphInfo) == 2 * 4 + 7 * 4
-    assert ctypes.sizeof(_lib.Config) == 19 * 4
+    assert ctypes.sizeof(_lib.Config) == 21 * 4
 
 
 def test_config_defaults_are_the_reference_defaults(monkeypatch):
