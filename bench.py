@@ -397,7 +397,7 @@ def run_batched(args):
     else:
         from mlmq_tpds_withl3_b200 import autotune
         bcfg, tune_report = autotune.tune_batch(queries, dg.slots)
-    batch = BatchSolver(len(srcs), dg.slots, bcfg)
+    batch = BatchSolver(len(srcs), dg.slots + (dg.n if bcfg.light_heavy else 0), bcfg)
     stream = torch.cuda.Stream()
 
     # Correctness: oracle on a few sources, the plain solver on every source.
@@ -524,7 +524,8 @@ def run_served(args):
         # pieces).  The server passes the settings with every query.
         from mlmq_tpds_withl3_b200 import autotune
         cands = [{"delta": d, "topup": t} for d in (50000, 100000, 200000) for t in (16, 32)]
-        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0}]
+        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0},
+                  {"delta": 50000, "topup": 32, "light_heavy": 1}]
         knobs, tune_report = [], {}
         base = {"warps_per_block": 8, "relax_unroll": 2}
         for i, dg in enumerate(dgs):
@@ -546,6 +547,8 @@ def run_served(args):
                              "qps_small_slots": qps_small, "qps_wide_slots": qps_wide}
             knobs.append(kc)
             tune_report[names[i]] = entry
+    if knobs is not None and any(k.light_heavy for k in knobs):
+        max_n = max(max_n, max(dg.slots + dg.n for dg, k in zip(dgs, knobs) if k.light_heavy))
     sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900, layout=layout)
     pool = PinnedPool(sv.slots, max_n)
     rates = [float(r) for r in args.rates.split(",")]

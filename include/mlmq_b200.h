@@ -107,11 +107,11 @@ typedef struct mlmq_config {
                             relaxations where buckets are wide and few
                             (power-law graphs), slower where they are many
                             (grids); default 0 */
-    int defer_degree;    /* >0: a vertex of at least this many arcs is relaxed
-                            one bucket late (a record for it re-enters at
-                            distance + delta), by then at its final distance,
-                            so hubs of power-law graphs are relaxed about
-                            once; needs vertex tiles and vertex slots
+    int light_heavy;     /* 1: delta-stepping's light/heavy split: a record
+                            relaxes its light arcs (weight < delta) at once
+                            and its heavy arcs one bucket later, when its
+                            distance is final, so heavy arcs are relaxed
+                            about once; needs vertex tiles, and vertex slots
                             n + pieces + n in batches and servers; default 0 */
     int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
                             32-byte tile (up to 4 arcs inline, else its CSR

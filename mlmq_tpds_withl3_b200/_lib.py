@@ -61,7 +61,7 @@ class Config(ctypes.Structure):
         "queue_type", "delta", "work_blocks", "warps_per_block", "l2_batch",
         "bucket_num", "bucket_max", "min_read", "large_degree", "l1_spill",
         "l2_cap_log2", "l3_cap_log2", "timeout_ms", "l1_keep", "relax_precheck",
-        "relax_unroll", "l1_ahead", "topup", "bucket_sync", "defer_degree", "vertex_tiles")]
+        "relax_unroll", "l1_ahead", "topup", "bucket_sync", "light_heavy", "vertex_tiles")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

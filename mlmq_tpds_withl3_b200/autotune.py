@@ -77,7 +77,7 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
     """Returns (config, report).  Candidates: delta from delta_candidates(),
     then warps per CTA in {8, 16, 24} at the best delta, then 1, 2 or 4
     relaxation rounds in flight, then vertex tiles on or off, then the L1
-    run-ahead bound."""
+    run-ahead bound, then the light/heavy split with bucket sync."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -113,6 +113,14 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         t = measure(over)
         if t < best_t:
             best, best_t = over, t
+    # The light/heavy split with bulk-synchronous buckets, at the best delta
+    # and a quarter of it (the split pays where many arcs are heavy).
+    if best.get("vertex_tiles", 1):
+        for dl in (best.get("delta", around), max(1, best.get("delta", around) // 4)):
+            over = {**best, "light_heavy": 1, "bucket_sync": 1, "delta": dl}
+            t = measure(over)
+            if t < best_t:
+                best, best_t = over, t
     report = {"key": key, "config": best, "seconds": best_t, "trials": results}
     if use_cache:
         store_cache(key, {"config": best, "seconds": best_t})
@@ -135,10 +143,14 @@ def tune_batch(queries, max_vertices, candidates=None, base=None):
                       for d in (50000, 100000, 200000) for t in (8, 16, 32)]
         candidates += [{"delta": 100000, "relax_unroll": 4, "topup": 16},
                        {"delta": 100000, "relax_unroll": 2, "topup": 16, "l1_ahead": 8},
-                       {"delta": 100000, "relax_unroll": 2}]
+                       {"delta": 100000, "relax_unroll": 2},
+                       {"delta": 50000, "relax_unroll": 2, "topup": 32, "light_heavy": 1}]
     results = []
+    n_max = max(g.n for g, _ in queries)
     for over in candidates:
-        b = BatchSolver(len(queries), max_vertices, {**base, **over})
+        # the light/heavy split needs n more vertex slots (heavy records)
+        mv = max_vertices + (n_max if over.get("light_heavy", base.get("light_heavy", 0)) else 0)
+        b = BatchSolver(len(queries), mv, {**base, **over})
         try:
             b.run(queries)  # warm-up
             t0 = time.perf_counter()

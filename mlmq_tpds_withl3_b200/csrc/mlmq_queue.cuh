@@ -56,7 +56,7 @@ namespace mlmq {
 struct PlainParams {
     int n;
     int nslots;  // n + split-vertex pieces (ids n .. nslots-1 are pieces)
-    int nids;    // nslots, + n when deferral is on (ids nslots + v: v's deferred record)
+    int nids;    // nslots, + n with the light/heavy split (ids nslots + v: v's heavy record)
     const int *__restrict__ row;
     const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
     const int4 *__restrict__ tiles; // 2 per vertex, or null: read row offsets instead
@@ -73,7 +73,7 @@ struct PlainParams {
     int l1_ahead;  // buckets past `first` a winner may be to stay in L1 (0: no limit)
     int topup;     // fewer than this many L1 records: fill the warp from L2 too
     int bucket_sync;  // 1: `first` advances only when no taken record is still in flight
-    int defer_deg;    // >0: vertices of at least this degree are relaxed one bucket late
+    const int *__restrict__ split;  // light arcs (w < delta) per vertex, or null: no split
     int precheck;  // read dist[dst] before the atomicMin
     unsigned delta;
     int l2_log, l3_log;
@@ -448,7 +448,7 @@ __device__ __forceinline__ int l3_rebucket(const PlainParams &p, WarpQ &q, volat
         atomicAnd(p.l3bits + (v >> 5), ~(1u << (v & 31u)));
         __threadfence();
         // A piece has no distance of its own: its owner's stands for it; a
-        // deferred record stands for its vertex's distance + delta.
+        // heavy record stands for its vertex's distance + delta.
         unsigned dv = v, add = 0u;
         if (v >= (unsigned)p.nslots) {
             dv = v - (unsigned)p.nslots;
@@ -602,10 +602,18 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
     int beg = 0, deg = 0;
     // Records are relaxed with their own distance: it is the length of a real
     // path, and with the fire-and-forget distance updates the update that
-    // made the record may not be visible here yet.  A deferred record (id
-    // nslots + v) carries v's distance + delta.
-    const bool deferred = valid && v >= (unsigned)p.nslots;
-    if (deferred) {
+    // made the record may not be visible here yet.
+    //
+    // Light/heavy split (p.split non-null; delta-stepping's light and heavy
+    // edges): arcs are sorted by weight, so a vertex's light arcs (w < delta)
+    // are a prefix.  A fresh record relaxes the light arcs at once and pushes
+    // one heavy record (id nslots + v) at distance + delta; heavy arcs cannot
+    // improve anything in the record's own bucket, and when the heavy record
+    // comes up the vertex's distance is (nearly always) final, so heavy arcs
+    // are relaxed about once.  A heavy record is fresh while the vertex's
+    // distance still equals the one it carries.
+    const bool heavyrec = valid && p.split && v >= (unsigned)p.nslots;
+    if (heavyrec) {
         v -= (unsigned)p.nslots;
         d -= p.delta;
     }
@@ -616,44 +624,75 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         // in the tile: they are staged in shared memory and its `beg` becomes
         // INT_MIN + its stage offset, so the arc distribution below handles
         // staged and CSR arcs alike and keeps the CSR path's arc order.
-        int cur = INT_MAX;
+        int cur = INT_MAX, light = 0;
         int4 ta = make_int4(-1, 0, -1, 0), tb = ta;
         const bool piece = valid && v >= (unsigned)p.n;
         if (valid) {
             if (!piece) cur = __ldcg(p.dist + v);
             ta = __ldg(p.tiles + 2 * (size_t)v);
             tb = __ldg(p.tiles + 2 * (size_t)v + 1);
+            if (p.split && !piece) light = __ldg(p.split + v);
         }
         if (piece) cur = __ldcg(p.dist + ta.w);  // a piece is as fresh as its owner
+        // Splitting needs room for distance + delta in a record.
+        const bool lh = p.split && !piece && d < (unsigned)INT_MAX - p.delta;
         int npieces = 0, first_piece = 0;
-        bool defer_now = false;
-        if (valid && (int)d <= cur && !deferred && !piece && p.defer_deg > 0) {
-            // A vertex of high degree waits one bucket: by the time the window
-            // reaches d + delta every improvement of its distance has arrived,
-            // so its (many) arcs are relaxed once, with the final distance.
-            const int vdeg = ta.x == TILE_CSR ? ta.z : (ta.x == TILE_SPLIT ? ta.w : 0);
-            defer_now = vdeg >= p.defer_deg && d < (unsigned)INT_MAX - p.delta;
-        }
-        if (valid && (int)d <= cur && !defer_now) {
+        bool push_heavy = false;
+        if (valid && (int)d <= cur) {
             if (ta.x == TILE_CSR) {
                 beg = ta.y;
                 deg = ta.z;
+                if (lh) {
+                    if (heavyrec) {
+                        beg += light;
+                        deg -= light;
+                    } else {
+                        deg = light;
+                        push_heavy = light < ta.z;
+                    }
+                }
             } else if (ta.x == TILE_SPLIT) {
                 first_piece = ta.y;
                 npieces = ta.z;
+                if (lh) {
+                    // pieces are cut every PIECE_ARCS sorted arcs: the first
+                    // nl hold every light arc
+                    const int nl = (light + PIECE_ARCS - 1) / PIECE_ARCS;
+                    if (heavyrec) {
+                        first_piece += nl;
+                        npieces -= nl;
+                    } else {
+                        npieces = nl;
+                        push_heavy = nl < ta.z;
+                    }
+                }
             } else {
                 int2 *st = stage + TILE_ARCS * lane;
                 st[0] = make_int2(ta.x, ta.y);
                 st[1] = make_int2(ta.z, ta.w);
                 st[2] = make_int2(tb.x, tb.y);
                 st[3] = make_int2(tb.z, tb.w);
-                deg = (ta.x >= 0) + (ta.z >= 0) + (tb.x >= 0) + (tb.z >= 0);
+                const int cnt = (ta.x >= 0) + (ta.z >= 0) + (tb.x >= 0) + (tb.z >= 0);
                 beg = INT_MIN + TILE_ARCS * lane;
+                deg = cnt;
+                if (lh) {
+                    // inline arcs are sorted by weight too
+                    const unsigned dl = p.delta;
+                    const int nl = (cnt > 0 && (unsigned)ta.y < dl) + (cnt > 1 && (unsigned)ta.w < dl) +
+                                   (cnt > 2 && (unsigned)tb.y < dl) + (cnt > 3 && (unsigned)tb.w < dl);
+                    if (heavyrec) {
+                        beg += nl;
+                        deg = cnt - nl;
+                    } else {
+                        deg = nl;
+                        push_heavy = nl < cnt;
+                    }
+                }
             }
         }
         if (__any_sync(FULL, npieces > 0)) push_pieces(p, q, npieces, first_piece, du);
-        if (__any_sync(FULL, defer_now))
-            push32(p, q, defer_now, (unsigned)p.nslots + v, d + p.delta);
+        if (__any_sync(FULL, push_heavy))
+            push32(p, q, push_heavy, (unsigned)p.nslots + v, d + p.delta);
         __syncwarp();
     } else if (valid) {
         // The three loads are independent: issue them together rather than

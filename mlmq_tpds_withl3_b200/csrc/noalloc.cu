@@ -166,7 +166,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.l1_ahead = cfg.l1_ahead;
     p.topup = cfg.topup;
     p.bucket_sync = cfg.bucket_sync;
-    p.defer_deg = 0;  // deferral needs vertex tiles
+    p.split = nullptr;  // the light/heavy split needs vertex tiles
     p.precheck = cfg.relax_precheck;
     p.delta = (unsigned)cfg.delta;
     p.l2_log = NA_L2_LOG;

@@ -2,6 +2,8 @@
 // context (distance array + queue workspace + persistent launch), the
 // reference-compatible entry points and the one-shot host-buffer call.
 #include "device_common.cuh"
+
+#include <cub/device/device_segmented_sort.cuh>
 #include "mlmq_b200.h"
 #include "mlmq_queue.cuh"
 #include "sssp_plain.h"
@@ -62,6 +64,22 @@ __global__ void tile_kernel(const int *__restrict__ row, const int2 *__restrict_
     }
 }
 
+// Light arcs (weight < delta) of each vertex: a lower bound search in its
+// weight-sorted arcs.
+__global__ void light_split_kernel(const int *__restrict__ row, const int2 *__restrict__ arcs, int n,
+                                   int delta, int *split) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int lo = row[v], hi = row[v + 1];
+        const int b = lo;
+        while (lo < hi) {
+            const int mid = lo + ((hi - lo) >> 1);
+            if (arcs[mid].y < delta) lo = mid + 1;
+            else hi = mid;
+        }
+        split[v] = lo - b;
+    }
+}
+
 // Heavy vertices' tiles: {TILE_SPLIT, first piece, pieces, degree}.
 __global__ void patch_tiles_kernel(const int *__restrict__ idx, const int4 *__restrict__ tile,
                                    int count, int4 *tiles) {
@@ -103,6 +121,31 @@ int env_int(const char *name, int dflt, bool *present) {
 
 }  // namespace
 
+int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
+    auto *g = const_cast<mlmq_graph *>(gc);
+    std::lock_guard<std::mutex> lk(g->split_mu);
+    for (auto &e : g->split_cache)
+        if (e.first == delta) {
+            *out = e.second;
+            return MLMQ_OK;
+        }
+    int *d = nullptr;
+    int rc = cuda_fail(cudaMalloc(&d, sizeof(int) * (size_t)g->n), "cudaMalloc(light split)");
+    if (!rc) {
+        const int blocks = (int)std::min<int64_t>(((int64_t)g->n + 255) / 256, 148 * 16);
+        light_split_kernel<<<blocks, 256>>>(g->d_row, g->d_arcs, g->n, delta, d);
+        rc = cuda_fail(cudaGetLastError(), "light split launch");
+        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "light split");
+    }
+    if (rc) {
+        cudaFree(d);
+        return rc;
+    }
+    g->split_cache.emplace_back(delta, d);
+    *out = d;
+    return MLMQ_OK;
+}
+
 int fill_device(int *p, int64_t n, int v, cudaStream_t s) {
     if (n <= 0) return MLMQ_OK;
     int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -135,7 +178,8 @@ int validate_config(const mlmq_config &c) {
     if (c.l1_ahead < 0) return MLMQ_ERR_ARG;
     if (c.topup < 0 || c.topup > 32) return MLMQ_ERR_ARG;
     if (c.bucket_sync != 0 && c.bucket_sync != 1) return MLMQ_ERR_ARG;
-    if (c.defer_degree < 0) return MLMQ_ERR_ARG;
+    if (c.light_heavy != 0 && c.light_heavy != 1) return MLMQ_ERR_ARG;
+    if (c.light_heavy && !c.vertex_tiles) return MLMQ_ERR_ARG;
     return MLMQ_OK;
 }
 
@@ -252,10 +296,30 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
     if (!rc) rc = cuda_fail(cudaMalloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1)),
                             "cudaMalloc(arcs)");
     if (!rc && m > 0) {
-        int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
-        interleave_kernel<<<blocks, 256>>>(d_col, d_w, g->d_arcs, m);
-        rc = cuda_fail(cudaGetLastError(), "interleave launch");
+        // Each vertex's arcs sorted by weight (light arcs, w < delta, then
+        // form a prefix for any delta), then interleaved.
+        int *k_out = nullptr, *v_out = nullptr;
+        void *tmp = nullptr;
+        size_t tmp_bytes = 0;
+        rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, d_w, k_out, d_col, v_out,
+                                                           (int)m, n, d_row, d_row + 1),
+                       "sort size");
+        if (!rc) rc = cuda_fail(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1), "cudaMalloc(sort)");
+        if (!rc) rc = cuda_fail(cudaMalloc(&k_out, sizeof(int) * (size_t)m), "cudaMalloc(sort keys)");
+        if (!rc) rc = cuda_fail(cudaMalloc(&v_out, sizeof(int) * (size_t)m), "cudaMalloc(sort values)");
+        if (!rc)
+            rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(tmp, tmp_bytes, d_w, k_out, d_col, v_out,
+                                                               (int)m, n, d_row, d_row + 1),
+                           "sort arcs");
+        if (!rc) {
+            int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
+            interleave_kernel<<<blocks, 256>>>(v_out, k_out, g->d_arcs, m);
+            rc = cuda_fail(cudaGetLastError(), "interleave launch");
+        }
         if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "interleave");
+        cudaFree(tmp);
+        cudaFree(k_out);
+        cudaFree(v_out);
     }
     // Heavy vertices and their pieces, from the row offsets.
     std::vector<int> heavy;           // vertex ids
@@ -380,6 +444,7 @@ extern "C" void mlmq_graph_free(mlmq_graph *g) {
     if (!g) return;
     if (g->d_arcs) cudaFree(g->d_arcs);
     if (g->d_tiles) cudaFree(g->d_tiles);
+    for (auto &e : g->split_cache) cudaFree(e.second);
     if (g->own_row && g->d_row) cudaFree(g->d_row);
     delete g;
 }
@@ -405,7 +470,11 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     const uint64_t m = (uint64_t)std::max<int64_t>(g->m, 1);
     s->l2_log = cfg.l2_cap_log2 ? cfg.l2_cap_log2
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
-    s->nids = g->slots() + (cfg.defer_degree ? g->n : 0);
+    s->nids = g->slots() + (cfg.light_heavy ? g->n : 0);
+    if (cfg.light_heavy && (rc = graph_light_split(g, cfg.delta, &s->split))) {
+        delete s;
+        return rc;
+    }
     s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(s->nids, g->m);
     s->workers = cfg.warps_per_block;
     int bps = 0;
@@ -485,7 +554,7 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.l1_ahead = s->cfg.l1_ahead;
     p.topup = s->cfg.topup;
     p.bucket_sync = s->cfg.bucket_sync;
-    p.defer_deg = s->cfg.defer_degree;
+    p.split = s->split;
     p.precheck = s->cfg.relax_precheck;
     p.delta = (unsigned)s->cfg.delta;
     p.l2_log = s->l2_log;

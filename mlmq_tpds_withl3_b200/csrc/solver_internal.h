@@ -4,6 +4,9 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "mlmq_b200.h"
 
@@ -17,6 +20,9 @@ struct mlmq_graph {
     int4 *d_tiles = nullptr; // 2 per vertex and per piece: the vertex tiles (always owned)
     int pieces = 0;          // virtual vertices n .. n + pieces - 1 (split heavy vertices)
     int slots() const { return n + pieces; }
+    // Per delta: light arcs (weight < delta) of each vertex, n ints.
+    std::mutex split_mu;
+    std::vector<std::pair<int, int *>> split_cache;
 };
 
 struct mlmq_solver {
@@ -25,7 +31,8 @@ struct mlmq_solver {
     int device = 0;
     int grid = 0, workers = 0;
     int l2_log = 0, l3_log = 0;
-    int nids = 0;               // queue ids: vertex slots, + n with deferral
+    int nids = 0;               // queue ids: vertex slots, + n with the light/heavy split
+    const int *split = nullptr; // light arcs per vertex for cfg.delta (owned by the graph)
     int *d_dist = nullptr;
     unsigned long long *d_l2 = nullptr;
     unsigned long long *d_l3 = nullptr;
@@ -42,6 +49,9 @@ namespace mlmq {
 
 int cuda_fail(cudaError_t e, const char *what);
 int fill_device(int *p, int64_t n, int v, cudaStream_t s);
+// Light arcs (weight < delta) of each vertex of g, computed once per delta
+// and kept with the graph.
+int graph_light_split(const mlmq_graph *g, int delta, const int **out);
 int validate_config(const mlmq_config &c);
 int status_to_error(unsigned st);
 int device_sm_count(int *sms);

@@ -37,6 +37,7 @@ struct BatchQuery {
     const int *row;
     const int2 *arcs;
     const int4 *tiles;
+    const int *split;
     int n, nslots, nids, src;
 };
 struct BatchParams {
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_batch_kernel(BatchP
     p.n = qy.n;
     p.nslots = qy.nslots;
     p.nids = qy.nids;
+    p.split = qy.split;
     p.src = qy.src;
     p.dist = bp.base.dist + s * bp.dist_stride;
     p.l2 = bp.base.l2 + s * bp.l2_stride;
@@ -159,7 +161,7 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     p.l1_ahead = b->cfg.l1_ahead;
     p.topup = b->cfg.topup;
     p.bucket_sync = b->cfg.bucket_sync;
-    p.defer_deg = b->cfg.defer_degree;
+    p.split = nullptr;  // per query
     p.precheck = b->cfg.relax_precheck;
     p.delta = (unsigned)b->cfg.delta;
     p.l2_log = b->l2_log;
@@ -261,7 +263,7 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
     if (!b || nq < 1 || nq > b->max_q || !graphs || !srcs) return MLMQ_ERR_ARG;
     for (int q = 0; q < nq; q++) {
         if (!graphs[q] || srcs[q] < 0 || srcs[q] >= graphs[q]->n ||
-            graphs[q]->slots() + (b->cfg.defer_degree ? graphs[q]->n : 0) > b->max_n)
+            graphs[q]->slots() + (b->cfg.light_heavy ? graphs[q]->n : 0) > b->max_n)
             return MLMQ_ERR_ARG;
         if (graphs[q]->device != b->device) return MLMQ_ERR_ARG;
     }
@@ -279,7 +281,9 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         qy.tiles = b->cfg.vertex_tiles ? g->d_tiles : nullptr;
         qy.n = g->n;
         qy.nslots = g->slots();
-        qy.nids = g->slots() + (b->cfg.defer_degree ? g->n : 0);
+        qy.nids = g->slots() + (b->cfg.light_heavy ? g->n : 0);
+        qy.split = nullptr;
+        if (b->cfg.light_heavy && (rc = graph_light_split(g, b->cfg.delta, &qy.split))) return rc;
         qy.src = srcs[q];
         b->n_of[q] = g->n;
         key.push_back((long long)(uintptr_t)g);

@@ -38,9 +38,9 @@ namespace {
 constexpr int SRV_CTL_STRIDE = 512;  // words per slot control block
 // Words of the slot control block used by the server around a solve (the
 // solve itself uses words below ctl::WORDS).
-constexpr int SRV_CMD = 464;      // device copy of the command: row, arcs, tiles (2 words each),
+constexpr int SRV_CMD = 456;      // device copy of the command: row, arcs, tiles (2 words each),
                                   // n, src, delta, topup, l1_ahead, bucket_max, nslots,
-                                  // bucket_sync, nids, defer_degree
+                                  // bucket_sync, nids, split (2 words)
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_BAR_COUNT = 488;
@@ -64,7 +64,8 @@ struct alignas(64) SlotCommand {
     int nslots, nids;
     // per-query settings (the server's configuration unless overridden)
     unsigned delta;
-    int topup, l1_ahead, bm, bucket_sync, defer_deg;
+    int topup, l1_ahead, bm, bucket_sync;
+    const int *split;
 };
 // Host-mapped completion, one per slot, written by the device.
 struct alignas(64) SlotCompletion {
@@ -168,7 +169,9 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                         c[SRV_CMD + 12] = (unsigned)sp.cmd[s].nslots;
                         c[SRV_CMD + 13] = (unsigned)sp.cmd[s].bucket_sync;
                         c[SRV_CMD + 14] = (unsigned)sp.cmd[s].nids;
-                        c[SRV_CMD + 15] = (unsigned)sp.cmd[s].defer_deg;
+                        const unsigned long long spl = (unsigned long long)sp.cmd[s].split;
+                        c[SRV_CMD + 15] = (unsigned)spl;
+                        c[SRV_CMD + 16] = (unsigned)(spl >> 32);
                         __threadfence();
                         // publish the sequence number (low 32 bits) to the group
                         st_release(c + SRV_GO, (unsigned)q);
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         p.nslots = (int)cmd[12];
         p.bucket_sync = (int)cmd[13];
         p.nids = (int)cmd[14];
-        p.defer_deg = (int)cmd[15];
+        p.split = (const int *)(((unsigned long long)cmd[16] << 32) | cmd[15]);
         p.n = (int)cmd[4];
         p.src = (int)cmd[5];
         p.dist = sp.dist + (size_t)s * sp.max_n;
@@ -418,7 +421,7 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
         b.l1_ahead = cfg.l1_ahead;
         b.topup = cfg.topup;
         b.bucket_sync = cfg.bucket_sync;
-        b.defer_deg = cfg.defer_degree;
+        b.split = nullptr;  // per query
         b.precheck = cfg.relax_precheck;
         b.delta = (unsigned)cfg.delta;
         b.l2_log = sv->l2_log;
@@ -506,8 +509,15 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     const mlmq_config &k = knobs ? *knobs : sv->cfg;
     if (k.delta < 1 || k.topup < 0 || k.topup > 32 || k.l1_ahead < 0 || k.bucket_max < 1 ||
         k.bucket_max > sv->cfg.bucket_num || (k.bucket_sync != 0 && k.bucket_sync != 1) ||
-        k.defer_degree < 0 || g->slots() + (k.defer_degree ? g->n : 0) > sv->max_n)
+        (k.light_heavy != 0 && k.light_heavy != 1) || (k.light_heavy && !sv->cfg.vertex_tiles) ||
+        g->slots() + (k.light_heavy ? g->n : 0) > sv->max_n)
         return MLMQ_ERR_ARG;
+    // Light arcs of this graph for this query's delta (computed on first use).
+    const int *split = nullptr;
+    if (k.light_heavy) {
+        const int rc = graph_light_split(g, k.delta, &split);
+        if (rc) return rc;
+    }
     // The smallest free slot with at least the CTAs the query asks for
     // (knobs->work_blocks; 0 or no knobs: any).
     const int want = knobs ? knobs->work_blocks : 0;
@@ -532,8 +542,8 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     cmd.l1_ahead = k.l1_ahead;
     cmd.bm = k.bucket_max;
     cmd.bucket_sync = k.bucket_sync;
-    cmd.defer_deg = k.defer_degree;
-    cmd.nids = g->slots() + (k.defer_degree ? g->n : 0);
+    cmd.split = split;
+    cmd.nids = g->slots() + (k.light_heavy ? g->n : 0);
     std::atomic_thread_fence(std::memory_order_release);
     sl.seq++;
     sl.busy = true;

@@ -84,8 +84,9 @@ def test_c1_grid512_bit_exact():
     {"l1_ahead": 1, "delta": 2000},
     {"bucket_sync": 1},
     {"bucket_sync": 1, "bucket_max": 1, "l1_ahead": 1, "delta": 3000},
-    {"defer_degree": 3},
-    {"defer_degree": 2, "bucket_sync": 1, "delta": 20000},
+    {"light_heavy": 1},
+    {"light_heavy": 1, "bucket_sync": 1, "bucket_max": 1, "delta": 20000},
+    {"light_heavy": 1, "delta": 1},
 ])
 def test_queue_configurations(cfg):
     """Any queue configuration gives the same exact distances (ordering only
@@ -129,15 +130,17 @@ def test_split_heavy_vertices_exact():
     # narrow buckets push pieces through L3 as well
     t = Solver(dg, {"bucket_num": 2, "bucket_max": 1, "delta": 3000, "timeout_ms": 15000})
     assert np.array_equal(t.solve(0).dist(), ref[0])
-    # deferred high-degree vertices (records re-enter at distance + delta),
+    # light/heavy split (heavy arcs and heavy pieces one bucket later),
     # single and batched, also through narrow buckets and L3
-    dfr = Solver(dg, {"defer_degree": 16})
-    for k, src in enumerate(srcs):
-        assert np.array_equal(dfr.solve(src).dist(), ref[k]), src
-    t2 = Solver(dg, {"defer_degree": 8, "bucket_num": 2, "bucket_max": 1, "delta": 3000,
+    for cfg in ({"light_heavy": 1}, {"light_heavy": 1, "delta": 20000, "bucket_sync": 1,
+                                     "bucket_max": 1}):
+        lh = Solver(dg, cfg)
+        for k, src in enumerate(srcs):
+            assert np.array_equal(lh.solve(src).dist(), ref[k]), (cfg, src)
+    t2 = Solver(dg, {"light_heavy": 1, "bucket_num": 2, "bucket_max": 1, "delta": 3000,
                      "timeout_ms": 15000})
     assert np.array_equal(t2.solve(1).dist(), ref[1])
-    bd = BatchSolver(len(srcs), dg.slots + dg.n, {"defer_degree": 16, "topup": 16})
+    bd = BatchSolver(len(srcs), dg.slots + dg.n, {"light_heavy": 1, "topup": 16})
     bd.run([(dg, x) for x in srcs])
     for k in range(len(srcs)):
         assert np.array_equal(bd.dist(k), ref[k])
