@@ -550,7 +550,7 @@ def run_served(args):
     if knobs is not None and any(k.light_heavy for k in knobs):
         max_n = max(max_n, max(dg.slots + dg.n for dg, k in zip(dgs, knobs) if k.light_heavy))
     sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900, layout=layout)
-    pool = PinnedPool(sv.slots, max_n)
+    pool = PinnedPool(sv.slots, max(ns))  # result buffers hold real vertices only
     rates = [float(r) for r in args.rates.split(",")]
     sweep = []
     sample = {}
