@@ -508,7 +508,7 @@ def run_served(args):
     ns = [hgs[k].n for k in names]
     max_n = max(dg.slots for dg in dgs)
     tune_report = None
-    cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2)
+    cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2, l2_cap_log2=20)
     knobs = None
     layout = None
     grid_max = 3 * 148  # CTAs of 8+1 warps that fit a B200 (the server checks)
@@ -524,10 +524,11 @@ def run_served(args):
         # pieces).  The server passes the settings with every query.
         from mlmq_tpds_withl3_b200 import autotune
         cands = [{"delta": d, "topup": t} for d in (50000, 100000, 200000) for t in (16, 32)]
-        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0},
-                  {"delta": 50000, "topup": 32, "light_heavy": 1}]
+        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0}]
+        cands += [{"delta": d, "topup": 32, "light_heavy": 1, "bucket_sync": 1}
+                  for d in (50000, 100000)]
         knobs, tune_report = [], {}
-        base = {"warps_per_block": 8, "relax_unroll": 2}
+        base = {"warps_per_block": 8, "relax_unroll": 2, "l2_cap_log2": 20}
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
