@@ -71,6 +71,7 @@ def parse():
                     help="served: wide slots for throughput-bound graphs (0: all slots equal; "
                          "on the 8-graph mix equal slots measured best)")
     ap.add_argument("--wide-ctas", type=int, default=54, help="served: CTAs of a wide slot")
+    ap.add_argument("--slot-warps", type=int, default=8, help="served: worker warps per CTA")
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
     ap.add_argument("--side", type=int, default=0,
                     help="c4: grid side instead of 4896 (small cases for profiler captures)")
@@ -508,7 +509,8 @@ def run_served(args):
     ns = [hgs[k].n for k in names]
     max_n = max(dg.slots for dg in dgs)
     tune_report = None
-    cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2, l2_cap_log2=20)
+    cfg = default_config(delta=100000, warps_per_block=args.slot_warps, relax_unroll=2,
+                         l2_cap_log2=20)
     knobs = None
     layout = None
     grid_max = 3 * 148  # CTAs of 8+1 warps that fit a B200 (the server checks)
@@ -528,7 +530,7 @@ def run_served(args):
         cands += [{"delta": d, "topup": 32, "light_heavy": 1, "bucket_sync": 1}
                   for d in (50000, 100000)]
         knobs, tune_report = [], {}
-        base = {"warps_per_block": 8, "relax_unroll": 2, "l2_cap_log2": 20}
+        base = {"warps_per_block": args.slot_warps, "relax_unroll": 2, "l2_cap_log2": 20}
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
