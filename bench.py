@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--config", default="",
+                    help="c1-c3: JSON overrides of the solver configuration, used instead of "
+                         "tuning (reproducible profiler runs)")
     return ap.parse_args()
 
 
@@ -242,7 +245,9 @@ def run_mlmq(args):
     g, srcs = load_workload(args.workload, args.sources)
     dg = DeviceGraph.upload(g)
     tune_report = None
-    if args.workload == "c1" or args.no_tune:
+    if args.config:
+        cfg = default_config(**{"delta": 200000, **json.loads(args.config)})
+    elif args.workload == "c1" or args.no_tune:
         cfg = default_config(delta=200000)
     else:
         cfg, tune_report = autotune.tune(dg, g, srcs[:2], kind=args.workload, use_cache=False)
@@ -394,7 +399,9 @@ def run_batched(args):
     queries = [(dg, s) for s in srcs]
     tune_report = None
     if args.no_tune:
-        bcfg = default_config(delta=200000, warps_per_block=8)
+        # the configuration the batch tuner settles on for grids
+        bcfg = default_config(delta=50000, warps_per_block=8, relax_unroll=2, topup=32,
+                              l2_cap_log2=20)
     else:
         from mlmq_tpds_withl3_b200 import autotune
         bcfg, tune_report = autotune.tune_batch(queries, dg.slots)
