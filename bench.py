@@ -231,12 +231,8 @@ def run_mlmq(args):
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        pg = dist
+    from mlmq_tpds_withl3_b200.replicas import Replicas, whole_job_rate
+    rep = Replicas("nccl")
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
     from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, autotune, default_config
@@ -281,9 +277,8 @@ def run_mlmq(args):
 
     for _ in range(args.warmup):
         step(None)
-    if pg:
-        pg.barrier()
     torch.cuda.synchronize()
+    rep.barrier()
     events = []
     sampler = ClockSampler(local)
     with sampler:
@@ -292,16 +287,11 @@ def run_mlmq(args):
             step(events)
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall0
-    if pg:
-        pg.barrier()
+    rep.barrier()
     per_query_ms = np.array([a.elapsed_time(b) for a, b in events])
-    total_s = per_query_ms.sum() / 1e3
-    if pg:
-        t = torch.tensor([total_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = rep.max(per_query_ms.sum() / 1e3)
     work_step = float(np.sum(works))
-    gteps = world * work_step * args.steps / total_s / 1e9
+    gteps = whole_job_rate(work_step * args.steps, world, total_s) / 1e9
 
     # Roofline of the persistent kernel.
     bytes_q = 12.0 * np.asarray(works, np.float64) + 12.0 * reached.astype(np.float64)
@@ -326,12 +316,8 @@ def run_mlmq(args):
                   "mlmq_solve_host")
             if i:
                 walls.append(time.perf_counter() - t0)
-        e2e_s = float(np.sum(walls))
-        if pg:
-            t = torch.tensor([e2e_s], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": world * work_step * len(walls) / e2e_s / 1e9, "unit": "GTEPS",
+        e2e_s = rep.max(float(np.sum(walls)))
+        e2e = {"value": whole_job_rate(work_step * len(walls), world, e2e_s) / 1e9, "unit": "GTEPS",
                "h2d_bytes_per_step": int(4 * (g.n + 1) + 8 * g.m),
                "d2h_bytes_per_step": int(4 * g.n * len(srcs)),
                "ms_per_step": e2e_s / len(walls) * 1e3,
@@ -344,9 +330,7 @@ def run_mlmq(args):
                "sample": f"{len(srcs)} sources of the same workload, one after another, "
                          f"{wall:.1f} s"}
 
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    rep.close()
     if rank != 0:
         return 0
     clocks = sampler.summary()
@@ -363,7 +347,7 @@ def run_mlmq(args):
                    "l2_between_solves": "flushed (256 MiB write, outside the timed events)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "correct": bool(correct),
-        "qps": world * len(srcs) * args.steps / total_s,
+        "qps": whole_job_rate(len(srcs) * args.steps, world, total_s),
         "latency_ms": {"p50": float(np.percentile(per_query_ms, 50)),
                        "p99": float(np.percentile(per_query_ms, 99))},
         "work_per_step": int(work_step),
@@ -387,6 +371,8 @@ def run_batched(args):
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
+    from mlmq_tpds_withl3_b200.replicas import Replicas, whole_job_rate
+    rep = Replicas("nccl")
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
     from mlmq_tpds_withl3_b200 import BatchSolver, DeviceGraph, Solver, default_config
@@ -442,6 +428,7 @@ def run_batched(args):
         batch.launch(queries, use_graph=True, stream=stream.cuda_stream)
         batch.wait()
     torch.cuda.synchronize()
+    rep.barrier()
     events = []
     sampler = ClockSampler(local)
     with sampler:
@@ -454,10 +441,12 @@ def run_batched(args):
             batch.wait()
             events.append((e0, e1))
         torch.cuda.synchronize()
+    rep.barrier()
     step_ms = np.array([a.elapsed_time(b) for a, b in events])
-    total_s = step_ms.sum() / 1e3
-    qps = len(srcs) * args.steps / total_s
-    plain_qps = len(srcs) / (np.sum(plain_ms) / 1e3)
+    total_s = rep.max(step_ms.sum() / 1e3)
+    qps = whole_job_rate(len(srcs) * args.steps, world, total_s)
+    plain_qps = whole_job_rate(len(srcs), world, rep.max(np.sum(plain_ms) / 1e3))
+    rep.close()
     bytes_step = 12.0 * work_step + 12.0 * float(sum(reached))
     achieved = bytes_step * args.steps / total_s / 1e9
     peak, peak_kind = measured_peak()
@@ -507,6 +496,8 @@ def run_served(args):
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
+    from mlmq_tpds_withl3_b200.replicas import Replicas
+    rep = Replicas("nccl", timeout_s=1800)
     from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, default_config, workloads
     from mlmq_tpds_withl3_b200.server import (PinnedPool, Server, poisson_schedule,
                                               serve_poisson, summarize)
@@ -610,8 +601,13 @@ def run_served(args):
         s.close()
     plain_qps = 1e3 / float(np.mean(plain_ms))
     top = max(sweep, key=lambda s: s["qps"])
+    # replicas serve independent arrival streams: the whole job's rate is the
+    # sum of theirs (one sum per collective, same order on every rank)
+    top_qps = rep.sum(top["qps"])
+    plain_qps = rep.sum(plain_qps)
+    rep.close()
     line = {
-        "metric": SERVE_METRIC, "value": top["qps"], "unit": "queries/s", "n_gpus": world,
+        "metric": SERVE_METRIC, "value": top_qps, "unit": "queries/s", "n_gpus": world,
         "steps": len(rates), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generators)",
@@ -629,7 +625,7 @@ def run_served(args):
                                "ms_per_query_mean": float(np.mean(plain_ms)),
                                "ms_mean_by_graph": {k: float(np.mean(v))
                                                     for k, v in sorted(plain_by_graph.items())}},
-        "speedup_vs_plain_qps": top["qps"] / plain_qps,
+        "speedup_vs_plain_qps": top_qps / plain_qps,
         "correct": bool(correct),
         "checked_alone_vs_mix": len(sample),
     }
