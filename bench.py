@@ -550,6 +550,9 @@ def run_served(args):
             tune_report[names[i]] = entry
     if knobs is not None and any(k.light_heavy for k in knobs):
         max_n = max(max_n, max(dg.slots + dg.n for dg, k in zip(dgs, knobs) if k.light_heavy))
+        for dg, k in zip(dgs, knobs):
+            if k.light_heavy:
+                dg.prepare_light(k.delta)
     sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900, layout=layout)
     pool = PinnedPool(sv.slots, max(ns))  # result buffers hold real vertices only
     rates = [float(r) for r in args.rates.split(",")]

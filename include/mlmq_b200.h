@@ -216,6 +216,13 @@ int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m);
  * after the graph's n.  A batch or server solving this graph needs
  * max_vertices >= n + pieces. */
 int mlmq_graph_pieces(const mlmq_graph *g, int *pieces);
+/* Computes (once, kept with the graph) each vertex's number of light arcs
+ * (weight < delta) for the light/heavy split.  Solvers and batches do it on
+ * first use; a server cannot, because its persistent launch holds every SM:
+ * prepare every (graph, delta) its light_heavy queries use before creating
+ * the server (mlmq_server_submit_cfg returns MLMQ_ERR_STATE otherwise).
+ * Likewise bind graphs before a server starts on the same device. */
+int mlmq_graph_prepare_light(const mlmq_graph *g, int delta);
 void mlmq_graph_free(mlmq_graph *g);
 
 /* A solver owns one distance array and one queue workspace on the device

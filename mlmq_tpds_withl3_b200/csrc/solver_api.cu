@@ -121,6 +121,17 @@ int env_int(const char *name, int dflt, bool *present) {
 
 }  // namespace
 
+int graph_light_split_cached(const mlmq_graph *gc, int delta, const int **out) {
+    auto *g = const_cast<mlmq_graph *>(gc);
+    std::lock_guard<std::mutex> lk(g->split_mu);
+    for (auto &e : g->split_cache)
+        if (e.first == delta) {
+            *out = e.second;
+            return MLMQ_OK;
+        }
+    return MLMQ_ERR_STATE;
+}
+
 int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
     auto *g = const_cast<mlmq_graph *>(gc);
     std::lock_guard<std::mutex> lk(g->split_mu);
@@ -425,6 +436,12 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
     g->own_row = true;
     *out = g;
     return MLMQ_OK;
+}
+
+extern "C" int mlmq_graph_prepare_light(const mlmq_graph *g, int delta) {
+    if (!g || delta < 1) return MLMQ_ERR_ARG;
+    const int *d = nullptr;
+    return graph_light_split(g, delta, &d);
 }
 
 extern "C" int mlmq_graph_pieces(const mlmq_graph *g, int *pieces) {

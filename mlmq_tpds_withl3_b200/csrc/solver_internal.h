@@ -52,6 +52,8 @@ int fill_device(int *p, int64_t n, int v, cudaStream_t s);
 // Light arcs (weight < delta) of each vertex of g, computed once per delta
 // and kept with the graph.
 int graph_light_split(const mlmq_graph *g, int delta, const int **out);
+// The same when already computed, else MLMQ_ERR_STATE (launches nothing).
+int graph_light_split_cached(const mlmq_graph *g, int delta, const int **out);
 int validate_config(const mlmq_config &c);
 int status_to_error(unsigned st);
 int device_sm_count(int *sms);

@@ -512,10 +512,12 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
         (k.light_heavy != 0 && k.light_heavy != 1) || (k.light_heavy && !sv->cfg.vertex_tiles) ||
         g->slots() + (k.light_heavy ? g->n : 0) > sv->max_n)
         return MLMQ_ERR_ARG;
-    // Light arcs of this graph for this query's delta (computed on first use).
+    // Light arcs of this graph for this query's delta.  The running server
+    // holds every SM, so nothing can be computed now: they must have been
+    // prepared (mlmq_graph_prepare_light) before the server started.
     const int *split = nullptr;
     if (k.light_heavy) {
-        const int rc = graph_light_split(g, k.delta, &split);
+        const int rc = graph_light_split_cached(g, k.delta, &split);
         if (rc) return rc;
     }
     // The smallest free slot with at least the CTAs the query asks for

@@ -51,6 +51,11 @@ class DeviceGraph:
               "mlmq_graph_wrap_device")
         return cls(h.value, n, m)
 
+    def prepare_light(self, delta):
+        """Light-arc counts for the light/heavy split at this delta (needed
+        before a server that runs light_heavy queries on this graph starts)."""
+        check(lib.mlmq_graph_prepare_light(self._h, int(delta)), "mlmq_graph_prepare_light")
+
     def close(self):
         if self._h is not None and self._h.value:
             lib.mlmq_graph_free(self._h)

@@ -65,6 +65,34 @@ def test_per_query_settings_give_the_same_result():
         assert np.array_equal(b.numpy(), ref)
 
 
+def test_light_heavy_queries_need_prepared_counts():
+    """A running server holds every SM, so light/heavy queries need their
+    light-arc counts prepared before it starts; unprepared ones are refused
+    at once (no device work inside submit), prepared ones are exact."""
+    from mlmq_tpds_withl3_b200 import MlmqError, default_config
+    from mlmq_tpds_withl3_b200._lib import MLMQ_ERR_STATE
+    import torch
+    import time
+    g = HostGraph.rmat(13, seed=48)
+    dg = DeviceGraph.upload(g)
+    dg.prepare_light(20000)
+    sv = Server(slots=3, max_vertices=dg.slots + dg.n, lifetime_s=60)
+    buf = torch.empty(g.n, dtype=torch.int32, pin_memory=True)
+    with pytest.raises(MlmqError) as ei:
+        sv.submit(dg, 0, buf, default_config(light_heavy=1, delta=30000))
+    assert ei.value.code == MLMQ_ERR_STATE
+    tk = sv.submit(dg, 0, buf, default_config(light_heavy=1, bucket_sync=1, delta=20000))
+    done = {}
+    t0 = time.time()
+    while tk not in done and time.time() - t0 < 30:
+        for t, st in sv.poll():
+            done[t] = st
+    sv.close()
+    assert done.get(tk) == 0
+    ref, _ = oracle_lib.sssp_i32(g, 0)
+    assert np.array_equal(buf.numpy(), ref)
+
+
 def test_slot_layout_and_slot_choice():
     """Slots of different sizes: a query asking for 6 CTAs gets the wide slot
     and waits while it is taken; results stay exact."""
