@@ -203,6 +203,14 @@ void mlmq_hgraph_free(mlmq_host_graph *g);
 typedef struct mlmq_graph mlmq_graph;
 typedef struct mlmq_solver mlmq_solver;
 
+/* Device memory of graphs and solvers comes from a stream-ordered pool per
+ * device that keeps freed memory for the next graph or solver (no release
+ * threshold), so code that builds and drops them per call, as
+ * mlmq_solve_host does, maps device memory once.  This returns the pools'
+ * unused memory to the driver (e.g. before another allocator needs it);
+ * memory still in use is not affected. */
+int mlmq_release_cached(void);
+
 /* Copies a host CSR to the current device (pinned staging) and builds the
  * interleaved {dst, weight} arc array the kernels read. */
 int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,

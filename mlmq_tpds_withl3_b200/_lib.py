@@ -114,6 +114,7 @@ _sig("mlmq_graph_size", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_i64
 _sig("mlmq_graph_pieces", c_int, c_vp, ctypes.POINTER(c_int))
 _sig("mlmq_graph_prepare_light", c_int, c_vp, c_int)
 _sig("mlmq_graph_free", None, c_vp)
+_sig("mlmq_release_cached", c_int)
 _sig("mlmq_solver_create", c_int, c_vp, ctypes.POINTER(Config), ctypes.POINTER(c_vp))
 _sig("mlmq_solver_launch", c_int, c_vp, c_int, c_vp)
 _sig("mlmq_solver_wait", c_int, c_vp)

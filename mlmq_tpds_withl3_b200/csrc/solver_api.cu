@@ -33,6 +33,91 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 namespace {
 
+// One pool per device, created on first use.  A release threshold of "all"
+// keeps freed blocks mapped for the next allocation of the process.
+std::mutex g_pool_mu;
+std::vector<cudaMemPool_t> g_pools;
+
+int device_pool(cudaMemPool_t *out) {
+    int dev = 0;
+    int rc = cuda_fail(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if ((int)g_pools.size() <= dev) g_pools.resize((size_t)dev + 1, nullptr);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        rc = cuda_fail(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        if (rc) return rc;
+        uint64_t keep = UINT64_MAX;
+        rc = cuda_fail(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                       "pool release threshold");
+        if (rc) {
+            cudaMemPoolDestroy(pool);
+            return rc;
+        }
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return MLMQ_OK;
+}
+
+// Page-locked copies of solver control blocks, carved from slabs of 64 that
+// are kept for reuse: page-locking memory per solver costs more than the
+// rest of creating one.
+constexpr int CTL_SLAB = 64;
+std::mutex g_pin_mu;
+std::vector<unsigned *> g_pin_free;
+
+}  // namespace
+
+int pinned_ctl_alloc(unsigned **p) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) {
+        unsigned *slab = nullptr;
+        const int rc = cuda_fail(cudaHostAlloc(&slab, sizeof(unsigned) * ctl::WORDS * CTL_SLAB,
+                                               cudaHostAllocPortable),
+                                 "pinned ctl");
+        if (rc) return rc;
+        for (int i = CTL_SLAB - 1; i >= 0; i--) g_pin_free.push_back(slab + (size_t)i * ctl::WORDS);
+    }
+    *p = g_pin_free.back();
+    g_pin_free.pop_back();
+    return MLMQ_OK;
+}
+
+void pinned_ctl_free(unsigned *p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+
+int dev_alloc(void **p, size_t bytes, cudaStream_t st, const char *what) {
+    *p = nullptr;
+    cudaMemPool_t pool = nullptr;
+    int rc = device_pool(&pool);
+    if (rc) return rc;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, st);
+    if (e == cudaErrorMemoryAllocation) {
+        // The pool's free blocks may be too small or fragmented: give them
+        // back to the driver and try once more.
+        cudaGetLastError();
+        cudaStreamSynchronize(st);
+        cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, st);
+    }
+    return cuda_fail(e, what);
+}
+
+void dev_free(const void *p, cudaStream_t st) {
+    if (p) cudaFreeAsync(const_cast<void *>(p), st);
+}
+
+namespace {
+
 __global__ void interleave_kernel(const int *__restrict__ col, const int *__restrict__ w, int2 *arcs,
                                   int64_t m) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
@@ -66,6 +151,18 @@ __global__ void tile_kernel(const int *__restrict__ row, const int2 *__restrict_
 
 // Light arcs (weight < delta) of each vertex: a lower bound search in its
 // weight-sorted arcs.
+// Vertices of more than SPLIT_MIN arcs as {vertex, first arc, degree, 0}, in
+// no particular order; *count may exceed cap only for invalid row offsets.
+__global__ void heavy_kernel(const int *__restrict__ row, int n, int *count, int4 *out, int cap) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int beg = row[v], deg = row[v + 1] - beg;
+        if (deg > SPLIT_MIN) {
+            const int k = atomicAdd(count, 1);
+            if (k < cap) out[k] = make_int4(v, beg, deg, 0);
+        }
+    }
+}
+
 __global__ void light_split_kernel(const int *__restrict__ row, const int2 *__restrict__ arcs, int n,
                                    int delta, int *split) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
@@ -141,7 +238,7 @@ int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
             return MLMQ_OK;
         }
     int *d = nullptr;
-    int rc = cuda_fail(cudaMalloc(&d, sizeof(int) * (size_t)g->n), "cudaMalloc(light split)");
+    int rc = dev_alloc(&d, sizeof(int) * (size_t)g->n, 0, "alloc(light split)");
     if (!rc) {
         const int blocks = (int)std::min<int64_t>(((int64_t)g->n + 255) / 256, 148 * 16);
         light_split_kernel<<<blocks, 256>>>(g->d_row, g->d_arcs, g->n, delta, d);
@@ -149,7 +246,7 @@ int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
         if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "light split");
     }
     if (rc) {
-        cudaFree(d);
+        dev_free(d, 0);
         return rc;
     }
     g->split_cache.emplace_back(delta, d);
@@ -293,7 +390,7 @@ namespace {
 // `h_row`: the same row offsets in host memory when the caller has them
 // (saves copying them back to find the heavy vertices), else null.
 int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int *d_w,
-                const int *h_row, mlmq_graph **out) {
+                mlmq_graph **out) {
     if (!out || n <= 0 || m < 0 || m >= INT_MAX || !d_row || (m > 0 && (!d_col || !d_w)))
         return MLMQ_ERR_ARG;
     auto *g = new (std::nothrow) mlmq_graph;
@@ -303,9 +400,10 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
     g->d_row = const_cast<int *>(d_row);
     g->own_row = false;
     g->d_arcs = nullptr;
+    // Everything below is ordered on the legacy default stream; the graph is
+    // complete when this returns (one device synchronisation at the end).
     int rc = cuda_fail(cudaGetDevice(&g->device), "cudaGetDevice");
-    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1)),
-                            "cudaMalloc(arcs)");
+    if (!rc) rc = dev_alloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1), 0, "alloc(arcs)");
     if (!rc && m > 0) {
         // Each vertex's arcs sorted by weight (light arcs, w < delta, then
         // form a prefix for any delta), then interleaved.
@@ -315,9 +413,9 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
         rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, d_w, k_out, d_col, v_out,
                                                            (int)m, n, d_row, d_row + 1),
                        "sort size");
-        if (!rc) rc = cuda_fail(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1), "cudaMalloc(sort)");
-        if (!rc) rc = cuda_fail(cudaMalloc(&k_out, sizeof(int) * (size_t)m), "cudaMalloc(sort keys)");
-        if (!rc) rc = cuda_fail(cudaMalloc(&v_out, sizeof(int) * (size_t)m), "cudaMalloc(sort values)");
+        if (!rc) rc = dev_alloc(&tmp, tmp_bytes, 0, "alloc(sort)");
+        if (!rc) rc = dev_alloc(&k_out, sizeof(int) * (size_t)m, 0, "alloc(sort keys)");
+        if (!rc) rc = dev_alloc(&v_out, sizeof(int) * (size_t)m, 0, "alloc(sort values)");
         if (!rc)
             rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(tmp, tmp_bytes, d_w, k_out, d_col, v_out,
                                                                (int)m, n, d_row, d_row + 1),
@@ -327,50 +425,66 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
             interleave_kernel<<<blocks, 256>>>(v_out, k_out, g->d_arcs, m);
             rc = cuda_fail(cudaGetLastError(), "interleave launch");
         }
-        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "interleave");
-        cudaFree(tmp);
-        cudaFree(k_out);
-        cudaFree(v_out);
+        dev_free(tmp, 0);
+        dev_free(k_out, 0);
+        dev_free(v_out, 0);
     }
-    // Heavy vertices and their pieces, from the row offsets.
+    // Heavy vertices (more than SPLIT_MIN arcs) are found on the device; at
+    // most m / (SPLIT_MIN + 1) exist.  Their pieces are laid out on the host
+    // in vertex order.
+    std::vector<int4> heavy_list;     // {vertex, first arc, degree, 0}
+    if (!rc && m > SPLIT_MIN) {
+        const int cap = (int)(m / (SPLIT_MIN + 1)) + 1;
+        int *d_count = nullptr;
+        int4 *d_list = nullptr;
+        int count = 0;
+        rc = dev_alloc(&d_count, sizeof(int), 0, "alloc(heavy count)");
+        if (!rc) rc = dev_alloc(&d_list, sizeof(int4) * (size_t)cap, 0, "alloc(heavy list)");
+        if (!rc) rc = cuda_fail(cudaMemsetAsync(d_count, 0, sizeof(int), 0), "heavy count");
+        if (!rc) {
+            const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 16);
+            heavy_kernel<<<blocks, 256>>>(d_row, n, d_count, d_list, cap);
+            rc = cuda_fail(cudaGetLastError(), "heavy launch");
+        }
+        if (!rc) rc = cuda_fail(cudaMemcpy(&count, d_count, sizeof(int), cudaMemcpyDeviceToHost),
+                                "D2H heavy count");
+        if (!rc && count > cap) rc = MLMQ_ERR_ARG;  // row offsets not monotone
+        if (!rc && count > 0) {
+            heavy_list.resize((size_t)count);
+            rc = cuda_fail(cudaMemcpy(heavy_list.data(), d_list, sizeof(int4) * (size_t)count,
+                                      cudaMemcpyDeviceToHost),
+                           "D2H heavy list");
+            std::sort(heavy_list.begin(), heavy_list.end(),
+                      [](const int4 &x, const int4 &y) { return x.x < y.x; });
+        }
+        dev_free(d_count, 0);
+        dev_free(d_list, 0);
+    }
     std::vector<int> heavy;           // vertex ids
     std::vector<int4> piece_tiles;    // 2 per piece
     std::vector<int4> heavy_tiles;    // 1 per heavy vertex (first half of its tile)
-    std::vector<int> row_copy;
-    const int *row = h_row;
-    if (!rc && !row) {
-        row_copy.resize((size_t)n + 1);
-        rc = cuda_fail(cudaMemcpy(row_copy.data(), d_row, sizeof(int) * ((size_t)n + 1),
-                                  cudaMemcpyDeviceToHost), "D2H row");
-        row = row_copy.data();
-    }
-    if (!rc) {
-        for (int v = 0; !rc && v < n; v++) {
-            const int deg = row[v + 1] - row[v];
-            if (deg <= SPLIT_MIN) continue;
-            const int np = (deg + PIECE_ARCS - 1) / PIECE_ARCS;
-            if ((int64_t)n + g->pieces + np >= INT_MAX) {
-                rc = MLMQ_ERR_RANGE;
-                break;
-            }
-            heavy.push_back(v);
-            heavy_tiles.push_back(make_int4(TILE_SPLIT, n + g->pieces, np, deg));
-            for (int k = 0; k < np; k++) {
-                const int b = row[v] + k * PIECE_ARCS;
-                const int c = std::min(PIECE_ARCS, row[v + 1] - b);
-                piece_tiles.push_back(make_int4(TILE_CSR, b, c, v));
-                piece_tiles.push_back(make_int4(-1, 0, -1, 0));
-            }
-            g->pieces += np;
+    for (size_t h = 0; !rc && h < heavy_list.size(); h++) {
+        const int v = heavy_list[h].x, beg = heavy_list[h].y, deg = heavy_list[h].z;
+        const int np = (deg + PIECE_ARCS - 1) / PIECE_ARCS;
+        if ((int64_t)n + g->pieces + np >= INT_MAX) {
+            rc = MLMQ_ERR_RANGE;
+            break;
         }
+        heavy.push_back(v);
+        heavy_tiles.push_back(make_int4(TILE_SPLIT, n + g->pieces, np, deg));
+        for (int k = 0; k < np; k++) {
+            const int b = beg + k * PIECE_ARCS;
+            const int c = std::min(PIECE_ARCS, beg + deg - b);
+            piece_tiles.push_back(make_int4(TILE_CSR, b, c, v));
+            piece_tiles.push_back(make_int4(-1, 0, -1, 0));
+        }
+        g->pieces += np;
     }
-    if (!rc) rc = cuda_fail(cudaMalloc(&g->d_tiles, 2 * sizeof(int4) * (size_t)g->slots()),
-                            "cudaMalloc(tiles)");
+    if (!rc) rc = dev_alloc(&g->d_tiles, 2 * sizeof(int4) * (size_t)g->slots(), 0, "alloc(tiles)");
     if (!rc) {
         int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 16);
         tile_kernel<<<blocks, 256>>>(d_row, g->d_arcs, g->d_tiles, n);
         rc = cuda_fail(cudaGetLastError(), "tile launch");
-        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "tiles");
     }
     if (!rc && g->pieces > 0) {
         rc = cuda_fail(cudaMemcpy(g->d_tiles + 2 * (size_t)n, piece_tiles.data(),
@@ -378,8 +492,8 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
                        "H2D piece tiles");
         int *d_idx = nullptr;
         int4 *d_ht = nullptr;
-        if (!rc) rc = cuda_fail(cudaMalloc(&d_idx, sizeof(int) * heavy.size()), "cudaMalloc(heavy)");
-        if (!rc) rc = cuda_fail(cudaMalloc(&d_ht, sizeof(int4) * heavy.size()), "cudaMalloc(heavy tiles)");
+        if (!rc) rc = dev_alloc(&d_idx, sizeof(int) * heavy.size(), 0, "alloc(heavy)");
+        if (!rc) rc = dev_alloc(&d_ht, sizeof(int4) * heavy.size(), 0, "alloc(heavy tiles)");
         if (!rc) rc = cuda_fail(cudaMemcpy(d_idx, heavy.data(), sizeof(int) * heavy.size(),
                                            cudaMemcpyHostToDevice), "H2D heavy");
         if (!rc) rc = cuda_fail(cudaMemcpy(d_ht, heavy_tiles.data(), sizeof(int4) * heavy.size(),
@@ -388,11 +502,11 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
             const int hn = (int)heavy.size();
             patch_tiles_kernel<<<(hn + 255) / 256, 256>>>(d_idx, d_ht, hn, g->d_tiles);
             rc = cuda_fail(cudaGetLastError(), "patch launch");
-            if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "patch tiles");
         }
-        cudaFree(d_idx);
-        cudaFree(d_ht);
+        dev_free(d_idx, 0);
+        dev_free(d_ht, 0);
     }
+    if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "graph build");
     if (rc) {
         mlmq_graph_free(g);
         return rc;
@@ -405,7 +519,7 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
 
 extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
                                       const int *d_w, mlmq_graph **out) {
-    return wrap_device(n, m, d_row, d_col, d_w, nullptr, out);
+    return wrap_device(n, m, d_row, d_col, d_w, out);
 }
 
 extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
@@ -414,9 +528,9 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
         return MLMQ_ERR_ARG;
     if (row[0] != 0 || row[n] != m) return MLMQ_ERR_ARG;
     int *d_row = nullptr, *d_col = nullptr, *d_w = nullptr;
-    int rc = cuda_fail(cudaMalloc(&d_row, sizeof(int) * ((size_t)n + 1)), "cudaMalloc(row)");
-    if (!rc && m > 0) rc = cuda_fail(cudaMalloc(&d_col, sizeof(int) * (size_t)m), "cudaMalloc(col)");
-    if (!rc && m > 0) rc = cuda_fail(cudaMalloc(&d_w, sizeof(int) * (size_t)m), "cudaMalloc(w)");
+    int rc = dev_alloc(&d_row, sizeof(int) * ((size_t)n + 1), 0, "alloc(row)");
+    if (!rc && m > 0) rc = dev_alloc(&d_col, sizeof(int) * (size_t)m, 0, "alloc(col)");
+    if (!rc && m > 0) rc = dev_alloc(&d_w, sizeof(int) * (size_t)m, 0, "alloc(w)");
     if (!rc) rc = cuda_fail(cudaMemcpy(d_row, row, sizeof(int) * ((size_t)n + 1),
                                        cudaMemcpyHostToDevice), "H2D row");
     if (!rc && m > 0)
@@ -426,11 +540,11 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
         rc = cuda_fail(cudaMemcpy(d_w, w, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
                        "H2D w");
     mlmq_graph *g = nullptr;
-    if (!rc) rc = wrap_device(n, m, d_row, d_col, d_w, row, &g);
-    if (d_col) cudaFree(d_col);
-    if (d_w) cudaFree(d_w);
+    if (!rc) rc = wrap_device(n, m, d_row, d_col, d_w, &g);
+    dev_free(d_col, 0);
+    dev_free(d_w, 0);
     if (rc) {
-        if (d_row) cudaFree(d_row);
+        dev_free(d_row, 0);
         return rc;
     }
     g->own_row = true;
@@ -459,10 +573,13 @@ extern "C" int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m) {
 
 extern "C" void mlmq_graph_free(mlmq_graph *g) {
     if (!g) return;
-    if (g->d_arcs) cudaFree(g->d_arcs);
-    if (g->d_tiles) cudaFree(g->d_tiles);
-    for (auto &e : g->split_cache) cudaFree(e.second);
-    if (g->own_row && g->d_row) cudaFree(g->d_row);
+    // Work still reading the graph on any stream ends first (cudaFree's
+    // implicit synchronisation, kept for the pool's stream-ordered frees).
+    cudaDeviceSynchronize();
+    dev_free(g->d_arcs, 0);
+    dev_free(g->d_tiles, 0);
+    for (auto &e : g->split_cache) dev_free(e.second, 0);
+    if (g->own_row) dev_free(g->d_row, 0);
     delete g;
 }
 
@@ -506,12 +623,12 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
     const size_t l3_bytes = sizeof(unsigned long long) * ((size_t)1 << s->l3_log);
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
     if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming), "event");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_dist, sizeof(int) * (size_t)g->n), "cudaMalloc(dist)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l2, l2_bytes), "cudaMalloc(L2)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3, l3_bytes), "cudaMalloc(L3)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_l3bits, l3_bits_bytes(s->nids)), "cudaMalloc(L3 bits)");
-    if (!rc) rc = cuda_fail(cudaMalloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS), "cudaMalloc(ctl)");
-    if (!rc) rc = cuda_fail(cudaMallocHost(&s->h_ctl, sizeof(unsigned) * ctl::WORDS), "pinned ctl");
+    if (!rc) rc = dev_alloc(&s->d_dist, sizeof(int) * (size_t)g->n, s->stream, "alloc(dist)");
+    if (!rc) rc = dev_alloc(&s->d_l2, l2_bytes, s->stream, "alloc(L2)");
+    if (!rc) rc = dev_alloc(&s->d_l3, l3_bytes, s->stream, "alloc(L3)");
+    if (!rc) rc = dev_alloc(&s->d_l3bits, l3_bits_bytes(s->nids), s->stream, "alloc(L3 bits)");
+    if (!rc) rc = dev_alloc(&s->d_ctl, sizeof(unsigned) * ctl::WORDS, s->stream, "alloc(ctl)");
+    if (!rc) rc = pinned_ctl_alloc(&s->h_ctl);
     if (!rc) rc = fill_device(s->d_dist, g->n, INT_MAX, s->stream);
     if (!rc) rc = cuda_fail(cudaStreamSynchronize(s->stream), "solver init");
     if (rc) {
@@ -643,16 +760,27 @@ extern "C" int mlmq_solver_stats(mlmq_solver *s, mlmq_solve_stats *st) {
 
 extern "C" void mlmq_solver_destroy(mlmq_solver *s) {
     if (!s) return;
+    // The last launch may have gone to a caller's stream: it ends before the
+    // workspace goes back to the pool.
+    if (s->done) cudaEventSynchronize(s->done);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->d_dist) cudaFree(s->d_dist);
-    if (s->d_l2) cudaFree(s->d_l2);
-    if (s->d_l3) cudaFree(s->d_l3);
-    if (s->d_l3bits) cudaFree(s->d_l3bits);
-    if (s->d_ctl) cudaFree(s->d_ctl);
-    if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    dev_free(s->d_dist, s->stream);
+    dev_free(s->d_l2, s->stream);
+    dev_free(s->d_l3, s->stream);
+    dev_free(s->d_l3bits, s->stream);
+    dev_free(s->d_ctl, s->stream);
+    pinned_ctl_free(s->h_ctl);
     if (s->done) cudaEventDestroy(s->done);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+}
+
+extern "C" int mlmq_release_cached(void) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    int rc = MLMQ_OK;
+    for (cudaMemPool_t pool : g_pools)
+        if (pool && !rc) rc = cuda_fail(cudaMemPoolTrimTo(pool, 0), "cudaMemPoolTrimTo");
+    return rc;
 }
 
 extern "C" int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
@@ -663,11 +791,27 @@ extern "C" int mlmq_solve_host(int n, int64_t m, const int *row, const int *col,
     if (rc) return rc;
     mlmq_solver *s = nullptr;
     rc = mlmq_solver_create(g, cfg, &s);
+    // Two distance arrays: source k + 1 is solved into one while source k's
+    // distances are copied out of the other (copy engines, beside the
+    // persistent kernel).  The kernel's prologue initialises its array.
+    int *own = s ? s->d_dist : nullptr, *spare = nullptr;
+    if (!rc && nsrc > 1) rc = dev_alloc(&spare, sizeof(int) * (size_t)n, s->stream, "alloc(dist)");
+    if (!rc && nsrc > 0) rc = mlmq_solver_launch(s, srcs[0], nullptr);
     for (int k = 0; !rc && k < nsrc; k++) {
-        rc = mlmq_solver_solve(s, srcs[k]);
-        if (!rc) rc = mlmq_solver_copy_dist(s, h_dist + (size_t)k * (size_t)n);
+        rc = mlmq_solver_wait(s);
+        int *solved = s->d_dist;
+        if (!rc && k + 1 < nsrc) {
+            s->d_dist = solved == own ? spare : own;
+            rc = mlmq_solver_launch(s, srcs[k + 1], nullptr);
+        }
+        if (!rc)
+            rc = cuda_fail(cudaMemcpy(h_dist + (size_t)k * (size_t)n, solved, sizeof(int) * (size_t)n,
+                                      cudaMemcpyDeviceToHost),
+                           "D2H dist");
     }
-    mlmq_solver_destroy(s);
+    if (s) s->d_dist = own;
+    mlmq_solver_destroy(s);  // waits for a launch still in flight after an error
+    dev_free(spare, 0);
     mlmq_graph_free(g);
     return rc;
 }

@@ -48,6 +48,20 @@ struct mlmq_solver {
 namespace mlmq {
 
 int cuda_fail(cudaError_t e, const char *what);
+// Device buffers of graphs and solvers: from this device's stream-ordered
+// pool (freed memory stays in the pool for reuse), ordered on `st`.
+int dev_alloc(void **p, size_t bytes, cudaStream_t st, const char *what);
+template <class T>
+int dev_alloc(T **p, size_t bytes, cudaStream_t st, const char *what) {
+    void *v = nullptr;
+    const int rc = dev_alloc(&v, bytes, st, what);
+    *p = static_cast<T *>(v);
+    return rc;
+}
+void dev_free(const void *p, cudaStream_t st);
+// One page-locked control-block copy (ctl::WORDS words) from a reused slab.
+int pinned_ctl_alloc(unsigned **p);
+void pinned_ctl_free(unsigned *p);
 int fill_device(int *p, int64_t n, int v, cudaStream_t s);
 // Light arcs (weight < delta) of each vertex of g, computed once per delta
 // and kept with the graph.

@@ -146,6 +146,55 @@ def test_split_heavy_vertices_exact():
         assert np.array_equal(bd.dist(k), ref[k])
 
 
+def test_graph_build_paths_and_pooled_memory():
+    """Graphs built from host arrays and from device arrays find the same
+    heavy vertices (found on the device) and solve exactly; graphs and
+    solvers built and dropped over and over reuse pooled device memory, and
+    releasing the pool's cache leaves live graphs and solvers intact."""
+    import torch
+    from mlmq_tpds_withl3_b200._lib import lib
+    g = HostGraph.rmat(15, seed=21)
+    ref, _ = oracle_lib.sssp_i32(g, 3)
+    up = DeviceGraph.upload(g)
+    row, col, w = (torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).cuda()
+                   for a in (g.row, g.col, g.w))
+    wrapped = DeviceGraph.wrap_device(g.n, g.m, row.data_ptr(), col.data_ptr(), w.data_ptr())
+    assert up.pieces > 0 and wrapped.pieces == up.pieces
+    live = Solver(wrapped)
+    assert np.array_equal(live.solve(3).dist(), ref)
+    for k in range(4):
+        dg = DeviceGraph.upload(g)
+        s = Solver(dg, {"light_heavy": k % 2})
+        assert np.array_equal(s.solve(3).dist(), ref), k
+        s.close()
+        dg.close()
+    assert lib.mlmq_release_cached() == 0
+    assert np.array_equal(live.solve(3).dist(), ref)
+    assert np.array_equal(Solver(up).solve(3).dist(), ref)
+
+
+def test_host_buffer_call_many_sources():
+    """mlmq_solve_host: upload, one solve per source (solving the next while
+    copying the last out), distances row by row; pageable and pinned output,
+    one source and none."""
+    import ctypes
+    import torch
+    from mlmq_tpds_withl3_b200 import solve_host, default_config
+    from mlmq_tpds_withl3_b200._lib import lib, check
+    g = HostGraph.rmat(14, seed=31)
+    srcs = [0, 7, 300, 7, 4095]
+    ref, _ = oracle_lib.sssp_many(g, srcs)
+    assert np.array_equal(solve_host(g, srcs), ref)
+    assert np.array_equal(solve_host(g, srcs[2:3], {"light_heavy": 1}), ref[2:3])
+    assert solve_host(g, []).shape == (0, g.n)
+    out = torch.empty((len(srcs), g.n), dtype=torch.int32).pin_memory()
+    sa = np.asarray(srcs, np.int32)
+    check(lib.mlmq_solve_host(g.n, g.m, g.row.ctypes.data, g.col.ctypes.data, g.w.ctypes.data,
+                              len(srcs), sa.ctypes.data, out.data_ptr(),
+                              ctypes.byref(default_config(vertex_tiles=0))), "mlmq_solve_host")
+    assert np.array_equal(out.numpy(), ref)
+
+
 def test_knn_and_rmat_medium():
     for g in (HostGraph.knn(200000, seed=2), HostGraph.rmat(16, seed=3)):
         s = Solver(DeviceGraph.upload(g))
