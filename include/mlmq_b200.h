@@ -342,6 +342,11 @@ int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int src,
 /* Advances finished queries (result copy-out) and reports up to `max`
  * completed tickets with their MLMQ_ERR_* status. */
 int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max, int *count);
+/* As mlmq_server_poll, with each query's device time in ns from its slot
+ * taking the command to the slot reporting the result (the solve without
+ * host-side queueing and result copy-out); solve_ns may be NULL. */
+int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *statuses,
+                           uint64_t *solve_ns, int max, int *count);
 int mlmq_server_busy_slots(mlmq_server *sv, int *busy);
 int mlmq_server_stop(mlmq_server *sv);
 void mlmq_server_destroy(mlmq_server *sv);

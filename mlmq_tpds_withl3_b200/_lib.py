@@ -150,6 +150,8 @@ _sig("mlmq_server_submit_cfg", c_int, c_vp, c_vp, c_int, ctypes.POINTER(Config),
      ctypes.POINTER(c_u64))
 _sig("mlmq_server_poll", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_int), c_int,
      ctypes.POINTER(c_int))
+_sig("mlmq_server_poll_timed", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_int),
+     ctypes.POINTER(c_u64), c_int, ctypes.POINTER(c_int))
 _sig("mlmq_server_busy_slots", c_int, c_vp, ctypes.POINTER(c_int))
 _sig("mlmq_server_stop", c_int, c_vp)
 _sig("mlmq_server_destroy", None, c_vp)

@@ -17,6 +17,7 @@ from ._lib import check, lib
 
 class BatchSolver:
     def __init__(self, max_queries, max_vertices, cfg=None):
+        self._h = None
         if cfg is None or isinstance(cfg, dict):
             over = {"warps_per_block": 8, **(cfg or {})}
             cfg = _lib.default_config(**over)

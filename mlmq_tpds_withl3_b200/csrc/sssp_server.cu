@@ -4,10 +4,15 @@
 //
 // The grid is split into `slots` contiguous CTA groups (as in the batched
 // launch).  Each slot owns a distance buffer, queue rings and a control
-// block.  The host hands a query to a free slot by writing a command into
-// pinned host memory that the GPU reads directly (mapped); the slot's first
-// CTA polls it, publishes it to the rest of its group in device memory, and
-// the group runs the single-source algorithm (sssp_plain_body.cuh).  At the
+// block.  The host hands a query to a free slot by copying a command into
+// the slot's mailbox in device memory (two small host-to-device copies on
+// their own stream: the fields, then the sequence number); the slot's first
+// CTA polls the mailbox, publishes the command to the rest of its group, and
+// the group runs the single-source algorithm (sssp_plain_body.cuh).  Idle
+// slots therefore poll HBM, not host memory: host-memory polling by dozens
+// of idle slots loaded PCIe enough to delay the result copies by ~200 ms,
+// which kept slots idle longer -- a feedback loop that held a 64-slot
+// server near 230 queries/s.  At the
 // end a group barrier makes sure every CTA of the slot has left the solve,
 // and the first CTA writes the completion (sequence number, status, counters)
 // into mapped host memory.  The host copies the distances out on another
@@ -46,14 +51,15 @@ constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_BAR_COUNT = 488;
 constexpr int SRV_BAR_GEN = 489;
 
-__device__ __forceinline__ unsigned long long ld_acquire_sys64(const volatile unsigned long long *p) {
+__device__ __forceinline__ unsigned long long ld_acquire64(const volatile unsigned long long *p) {
     unsigned long long v;
-    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
-// Host-mapped command, one per slot, written by the host: every field first,
-// then `seq` (x86 stores become visible in program order).
+// Command, one per slot: staged in pinned host memory, copied into the
+// slot's device mailbox -- every field first, then `seq` (a second copy in
+// the same stream, so the fields are in device memory before it lands).
 struct alignas(64) SlotCommand {
     volatile unsigned long long seq;
     const int *row;
@@ -73,13 +79,15 @@ struct alignas(64) SlotCompletion {
     volatile unsigned status;
     volatile unsigned first_max;
     volatile unsigned long long relaxed, pushed;
+    // device clock (ns): the slot took the command / reported the result
+    volatile unsigned long long t_start, t_end;
 };
 
 struct ServerParams {
     PlainParams base;             // queue configuration shared by all slots
-    SlotCommand *cmd;             // mapped, [slots]
+    SlotCommand *cmd;             // device mailboxes, [slots]
     SlotCompletion *done;         // mapped, [slots]
-    volatile unsigned *shutdown;  // mapped
+    volatile unsigned *shutdown;  // device
     int *dist;                    // slots * max_n
     unsigned long long *l2, *l3;
     unsigned *l3bits;             // slots * bits_words
@@ -132,7 +140,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
     const unsigned grank = blockIdx.x - lo, gsize = hi - lo;
     unsigned *c = sp.ctl + (size_t)s * SRV_CTL_STRIDE;
     const unsigned long long end = globaltimer() + sp.lifetime_ns;
-    __shared__ unsigned long long go_seq;
+    __shared__ unsigned long long go_seq, go_time;
     __shared__ int stop;
     unsigned long long seen = 0;
     for (;;) {
@@ -142,34 +150,36 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
             unsigned ns = 256;
             for (;;) {
                 if (grank == 0) {
-                    if (*sp.shutdown) {
+                    if (ld_acquire(const_cast<const unsigned *>(sp.shutdown))) {
                         st_release(c + SRV_STOP, 1u);
                         stop = 1;
                         break;
                     }
-                    const unsigned long long q = ld_acquire_sys64(&sp.cmd[s].seq);
+                    const unsigned long long q = ld_acquire64(&sp.cmd[s].seq);
                     if (q != seen) {
                         go_seq = q;
-                        // Copy the command into device memory for the group.
-                        const unsigned long long row = (unsigned long long)sp.cmd[s].row;
-                        const unsigned long long arcs = (unsigned long long)sp.cmd[s].arcs;
+                        go_time = globaltimer();
+                        // Copy the command into the control block for the group.
+                        const volatile SlotCommand &cm = sp.cmd[s];
+                        const unsigned long long row = (unsigned long long)cm.row;
+                        const unsigned long long arcs = (unsigned long long)cm.arcs;
                         c[SRV_CMD + 0] = (unsigned)row;
                         c[SRV_CMD + 1] = (unsigned)(row >> 32);
                         c[SRV_CMD + 2] = (unsigned)arcs;
                         c[SRV_CMD + 3] = (unsigned)(arcs >> 32);
-                        c[SRV_CMD + 4] = (unsigned)sp.cmd[s].n;
-                        c[SRV_CMD + 5] = (unsigned)sp.cmd[s].src;
-                        const unsigned long long tiles = (unsigned long long)sp.cmd[s].tiles;
+                        c[SRV_CMD + 4] = (unsigned)cm.n;
+                        c[SRV_CMD + 5] = (unsigned)cm.src;
+                        const unsigned long long tiles = (unsigned long long)cm.tiles;
                         c[SRV_CMD + 6] = (unsigned)tiles;
                         c[SRV_CMD + 7] = (unsigned)(tiles >> 32);
-                        c[SRV_CMD + 8] = sp.cmd[s].delta;
-                        c[SRV_CMD + 9] = (unsigned)sp.cmd[s].topup;
-                        c[SRV_CMD + 10] = (unsigned)sp.cmd[s].l1_ahead;
-                        c[SRV_CMD + 11] = (unsigned)sp.cmd[s].bm;
-                        c[SRV_CMD + 12] = (unsigned)sp.cmd[s].nslots;
-                        c[SRV_CMD + 13] = (unsigned)sp.cmd[s].bucket_sync;
-                        c[SRV_CMD + 14] = (unsigned)sp.cmd[s].nids;
-                        const unsigned long long spl = (unsigned long long)sp.cmd[s].split;
+                        c[SRV_CMD + 8] = cm.delta;
+                        c[SRV_CMD + 9] = (unsigned)cm.topup;
+                        c[SRV_CMD + 10] = (unsigned)cm.l1_ahead;
+                        c[SRV_CMD + 11] = (unsigned)cm.bm;
+                        c[SRV_CMD + 12] = (unsigned)cm.nslots;
+                        c[SRV_CMD + 13] = (unsigned)cm.bucket_sync;
+                        c[SRV_CMD + 14] = (unsigned)cm.nids;
+                        const unsigned long long spl = (unsigned long long)cm.split;
                         c[SRV_CMD + 15] = (unsigned)spl;
                         c[SRV_CMD + 16] = (unsigned)(spl >> 32);
                         __threadfence();
@@ -248,6 +258,8 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
             sp.done[s].first_max = (unsigned)u[ctl::ST_FIRST_MAX];
             sp.done[s].relaxed = u[ctl::ST_RELAXED];
             sp.done[s].pushed = u[ctl::ST_PUSHED];
+            sp.done[s].t_start = go_time;
+            sp.done[s].t_end = globaltimer();
             __threadfence_system();
             sp.done[s].seq = seen;
             __threadfence_system();
@@ -280,10 +292,13 @@ struct mlmq_server {
     unsigned *d_ctl = nullptr;
     int *d_cta_slot = nullptr, *d_slot_first = nullptr;
     std::vector<int> slot_ctas;   // CTAs of each slot
-    SlotCommand *h_cmd = nullptr;
+    SlotCommand *h_cmd = nullptr;   // pinned staging of each slot's command
+    SlotCommand *d_cmd = nullptr;   // device mailboxes
     SlotCompletion *h_done = nullptr;
-    unsigned *h_shutdown = nullptr;
+    unsigned *h_shutdown = nullptr; // pinned staging of the shutdown flag
+    unsigned *d_shutdown = nullptr;
     cudaStream_t kstream = nullptr, cstream = nullptr;
+    cudaStream_t qstream = nullptr;  // command and shutdown copies
     cudaEvent_t kdone = nullptr;
     bool running = false;
     std::mutex mu;
@@ -297,10 +312,16 @@ struct mlmq_server {
         cudaEvent_t copied = nullptr;
         unsigned status = 0;
         unsigned long long relaxed = 0;
+        unsigned long long solve_ns = 0;
     };
     std::vector<Slot> st;
     unsigned long long next_ticket = 1;
-    std::deque<std::pair<unsigned long long, int>> finished;  // (ticket, status)
+    struct Finished {
+        unsigned long long ticket;
+        int status;
+        unsigned long long solve_ns;  // device time from command pickup to result
+    };
+    std::deque<Finished> finished;
 };
 
 namespace {
@@ -390,11 +411,14 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3, 8 * (ns << sv->l3_log)), "server L3");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3bits, 4 * ns * sv->bits_words), "server L3 bits");
     if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_ctl, 4 * ns * SRV_CTL_STRIDE), "server ctl");
-    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_cmd, sizeof(SlotCommand) * ns, cudaHostAllocMapped), "cmd");
+    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_cmd, sizeof(SlotCommand) * ns, cudaHostAllocDefault), "cmd");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_cmd, sizeof(SlotCommand) * ns), "server mailboxes");
+    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_shutdown, 64), "server shutdown flag");
     if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_done, sizeof(SlotCompletion) * ns, cudaHostAllocMapped), "done");
-    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_shutdown, 64, cudaHostAllocMapped), "shutdown");
+    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_shutdown, 64, cudaHostAllocDefault), "shutdown");
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking), "kstream");
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "cstream");
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->qstream, cudaStreamNonBlocking), "qstream");
     if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&sv->kdone, cudaEventDisableTiming), "kdone");
     if (!rc) {
         std::memset((void *)sv->h_cmd, 0, sizeof(SlotCommand) * ns);
@@ -407,6 +431,8 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
     if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_l2, 0xff, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log), sv->kstream), "reset L2");
     if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_l3, 0xff, 8 * (ns << sv->l3_log), sv->kstream), "reset L3");
     if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_ctl, 0, 4 * ns * SRV_CTL_STRIDE, sv->kstream), "reset ctl");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_cmd, 0, sizeof(SlotCommand) * ns, sv->kstream), "reset mailboxes");
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(sv->d_shutdown, 0, 64, sv->kstream), "reset shutdown");
     if (!rc) {
         ServerParams sp{};
         PlainParams &b = sp.base;
@@ -428,13 +454,11 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
         b.l3_log = sv->l3_log;
         b.workers = sv->workers;
         b.timeout_ns = (unsigned long long)cfg.timeout_ms * 1000000ull;
-        void *p_cmd = nullptr, *p_done = nullptr, *p_stop = nullptr;
-        rc = cuda_fail(cudaHostGetDevicePointer(&p_cmd, sv->h_cmd, 0), "map cmd");
-        if (!rc) rc = cuda_fail(cudaHostGetDevicePointer(&p_done, sv->h_done, 0), "map done");
-        if (!rc) rc = cuda_fail(cudaHostGetDevicePointer(&p_stop, sv->h_shutdown, 0), "map stop");
-        sp.cmd = (SlotCommand *)p_cmd;
+        void *p_done = nullptr;
+        rc = cuda_fail(cudaHostGetDevicePointer(&p_done, sv->h_done, 0), "map done");
+        sp.cmd = sv->d_cmd;
         sp.done = (SlotCompletion *)p_done;
-        sp.shutdown = (volatile unsigned *)p_stop;
+        sp.shutdown = sv->d_shutdown;
         sp.dist = sv->d_dist;
         sp.l2 = sv->d_l2;
         sp.l3 = sv->d_l3;
@@ -553,7 +577,21 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     sl.ticket = sv->next_ticket++;
     sl.h_out = h_out;
     sl.n = g->n;
-    cmd.seq = sl.seq;  // published last
+    cmd.seq = sl.seq;
+    // Fields first, then the sequence number: in one stream the second copy
+    // starts after the first has landed.  The staging entry is not written
+    // again before the slot has taken this command (it is busy until then).
+    constexpr size_t head = sizeof(cmd.seq);
+    char *dst = reinterpret_cast<char *>(sv->d_cmd + free_slot);
+    const char *src_b = reinterpret_cast<const char *>(&cmd);
+    int rc = cuda_fail(cudaMemcpyAsync(dst + head, src_b + head, sizeof(SlotCommand) - head,
+                                       cudaMemcpyHostToDevice, sv->qstream), "command fields");
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(dst, src_b, head, cudaMemcpyHostToDevice, sv->qstream),
+                            "command sequence");
+    if (rc) {
+        sl.busy = false;
+        return rc;
+    }
     *ticket = sl.ticket;
     return MLMQ_OK;
 }
@@ -566,6 +604,11 @@ extern "C" int mlmq_server_submit(mlmq_server *sv, const mlmq_graph *g, int src,
 // Moves finished solves to the copy stream and retires finished copies.
 extern "C" int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max,
                                 int *count) {
+    return mlmq_server_poll_timed(sv, tickets, statuses, nullptr, max, count);
+}
+
+extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *statuses,
+                                      uint64_t *solve_ns, int max, int *count) {
     if (!sv || !count || (max > 0 && (!tickets || !statuses))) return MLMQ_ERR_ARG;
     std::lock_guard<std::mutex> lk(sv->mu);
     int rc = MLMQ_OK;
@@ -577,6 +620,7 @@ extern "C" int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuse
             std::atomic_thread_fence(std::memory_order_acquire);
             sl.status = sv->h_done[s].status;
             sl.relaxed = sv->h_done[s].relaxed;
+            sl.solve_ns = sv->h_done[s].t_end - sv->h_done[s].t_start;
             rc = cuda_fail(cudaMemcpyAsync(sl.h_out, sv->d_dist + (size_t)s * sv->max_n,
                                            sizeof(int) * (size_t)sl.n, cudaMemcpyDeviceToHost,
                                            sv->cstream), "server D2H");
@@ -586,13 +630,14 @@ extern "C" int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuse
         } else if (cudaEventQuery(sl.copied) == cudaSuccess) {
             sl.busy = false;
             sl.copying = false;
-            sv->finished.emplace_back(sl.ticket, status_to_error(sl.status));
+            sv->finished.push_back({sl.ticket, status_to_error(sl.status), sl.solve_ns});
         }
     }
     int k = 0;
     while (k < max && !sv->finished.empty()) {
-        tickets[k] = sv->finished.front().first;
-        statuses[k] = sv->finished.front().second;
+        tickets[k] = sv->finished.front().ticket;
+        statuses[k] = sv->finished.front().status;
+        if (solve_ns) solve_ns[k] = sv->finished.front().solve_ns;
         sv->finished.pop_front();
         k++;
     }
@@ -613,12 +658,17 @@ extern "C" int mlmq_server_busy_slots(mlmq_server *sv, int *busy) {
 
 extern "C" int mlmq_server_stop(mlmq_server *sv) {
     if (!sv) return MLMQ_ERR_ARG;
-    if (sv->h_shutdown) {
-        *(volatile unsigned *)sv->h_shutdown = 1;
-        std::atomic_thread_fence(std::memory_order_seq_cst);
-    }
     int rc = MLMQ_OK;
-    if (sv->kstream) rc = cuda_fail(cudaStreamSynchronize(sv->kstream), "server stop");
+    if (sv->h_shutdown && sv->d_shutdown && sv->qstream) {
+        *(volatile unsigned *)sv->h_shutdown = 1;
+        rc = cuda_fail(cudaMemcpyAsync(sv->d_shutdown, sv->h_shutdown, sizeof(unsigned),
+                                       cudaMemcpyHostToDevice, sv->qstream), "shutdown flag");
+        if (!rc) rc = cuda_fail(cudaStreamSynchronize(sv->qstream), "shutdown flag sync");
+    }
+    if (sv->kstream) {
+        const int krc = cuda_fail(cudaStreamSynchronize(sv->kstream), "server stop");
+        if (!rc) rc = krc;
+    }
     if (sv->cstream) cudaStreamSynchronize(sv->cstream);
     sv->running = false;
     return rc;
@@ -637,10 +687,13 @@ extern "C" void mlmq_server_destroy(mlmq_server *sv) {
     cudaFree(sv->d_cta_slot);
     cudaFree(sv->d_slot_first);
     if (sv->h_cmd) cudaFreeHost(sv->h_cmd);
+    cudaFree(sv->d_cmd);
+    cudaFree(sv->d_shutdown);
     if (sv->h_done) cudaFreeHost(sv->h_done);
     if (sv->h_shutdown) cudaFreeHost(sv->h_shutdown);
     if (sv->kdone) cudaEventDestroy(sv->kdone);
     if (sv->kstream) cudaStreamDestroy(sv->kstream);
     if (sv->cstream) cudaStreamDestroy(sv->cstream);
+    if (sv->qstream) cudaStreamDestroy(sv->qstream);
     delete sv;
 }

@@ -51,6 +51,7 @@ class Server:
         self.max_vertices = max_vertices
         self._tk = (ctypes.c_uint64 * 256)()
         self._st = (ctypes.c_int * 256)()
+        self._ns = (ctypes.c_uint64 * 256)()
 
     def submit(self, dgraph, src, out, knobs=None):
         """Returns a ticket, or None when every slot is busy.  `out` must be a
@@ -75,6 +76,14 @@ class Server:
         check(lib.mlmq_server_poll(self._h, self._tk, self._st, 256, ctypes.byref(n)),
               "mlmq_server_poll")
         return [(self._tk[i], self._st[i]) for i in range(n.value)]
+
+    def poll_timed(self):
+        """[(ticket, status, solve_ms)]: as poll, with each query's device time
+        from its slot taking the command to the slot reporting the result."""
+        n = ctypes.c_int()
+        check(lib.mlmq_server_poll_timed(self._h, self._tk, self._st, self._ns, 256,
+                                         ctypes.byref(n)), "mlmq_server_poll_timed")
+        return [(self._tk[i], self._st[i], self._ns[i] / 1e6) for i in range(n.value)]
 
     def busy(self):
         b = ctypes.c_int()
@@ -115,7 +124,7 @@ def poisson_schedule(rate, count, graphs_n, seed=1):
 
 def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0, knobs=None):
     """Runs the schedule against the server.  Returns a list of dicts
-    (arrival, start, finish, latency_s, graph, src, status[, dist]) in
+    (arrival, start, finish, latency_s, solve_ms, graph, src, status[, dist]) in
     schedule order; `keep(i)` selects the queries whose distances are kept;
     `knobs[graph index]` (optional) is that graph's per-query Config."""
     pool = pool or PinnedPool(server.slots, max(g.n for g in dgraphs))
@@ -157,12 +166,12 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
                 continue
             inflight[tk] = (i, buf, now)
         pending.extendleft(reversed(skipped))
-        for tk, status in server.poll():
+        for tk, status, solve_ms in server.poll_timed():
             i, buf, start = inflight.pop(tk)
             arr, gi, src = schedule[i]
             fin = time.perf_counter() - t0
             rec = {"arrival": arr, "start": start, "finish": fin, "latency_s": fin - arr,
-                   "graph": gi, "src": src, "status": status}
+                   "solve_ms": solve_ms, "graph": gi, "src": src, "status": status}
             if keep is not None and keep(i):
                 rec["dist"] = buf[:dgraphs[gi].n].numpy().copy()
             out[i] = rec
@@ -196,6 +205,7 @@ def summarize(records, names=None):
             gl = np.array([r["latency_s"] for r in sel]) * 1e3
             per[name] = {"queries": len(sel), "errors": sum(1 for r in sel if r["status"]),
                          "p50_ms": float(np.percentile(gl, 50)),
-                         "run_ms_mean": float(run.mean())}
+                         "run_ms_mean": float(run.mean()),
+                         "solve_ms_mean": float(np.mean([r["solve_ms"] for r in sel]))}
         out["per_graph"] = per
     return out

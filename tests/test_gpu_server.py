@@ -24,6 +24,8 @@ def test_served_results_equal_oracle_and_alone():
     recs = serve_poisson(sv, dgs, sched, keep=lambda i: True, timeout_s=60)
     sv.close()
     assert all(r["status"] == 0 for r in recs)
+    # device solve time: positive and inside the host-seen submit-to-result span
+    assert all(0 < r["solve_ms"] <= (r["finish"] - r["start"]) * 1e3 + 1.0 for r in recs)
     # queries overlapped on the device: some started before others finished
     overlap = sum(1 for a, b in zip(recs, recs[1:]) if b["start"] < a["finish"])
     assert overlap > 0
