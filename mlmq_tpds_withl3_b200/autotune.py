@@ -77,7 +77,9 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
     """Returns (config, report).  Candidates: delta from delta_candidates(),
     then warps per CTA in {8, 16, 24} at the best delta, then 1, 2 or 4
     relaxation rounds in flight, then vertex tiles on or off, then the L1
-    run-ahead bound, then the light/heavy split with bucket sync."""
+    run-ahead bound, then the light/heavy split with bucket sync, then L2
+    claims of 16 slots (they pay with the split on R-MAT, 5.4 -> 4.7 ms, and
+    cost narrow-frontier solves: kNN 10.5 -> 12.3 ms)."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -114,13 +116,22 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         if t < best_t:
             best, best_t = over, t
     # The light/heavy split with bulk-synchronous buckets, at the best delta
-    # and a quarter of it (the split pays where many arcs are heavy).
+    # and a quarter of it (the split pays where many arcs are heavy), on the
+    # shape found so far and on the default one: the stages above are
+    # greedy, and a shape picked without the split (more warps per CTA) can
+    # be the wrong one with it.
     if best.get("vertex_tiles", 1):
-        for dl in (best.get("delta", around), max(1, best.get("delta", around) // 4)):
-            over = {**best, "light_heavy": 1, "bucket_sync": 1, "delta": dl}
-            t = measure(over)
-            if t < best_t:
-                best, best_t = over, t
+        shapes = [best, {"delta": best["delta"]}]
+        for shape in shapes[:1] if shapes[0] == shapes[1] else shapes:
+            for dl in (shape["delta"], max(1, shape["delta"] // 4)):
+                over = {**shape, "light_heavy": 1, "bucket_sync": 1, "delta": dl}
+                t = measure(over)
+                if t < best_t:
+                    best, best_t = over, t
+    over = {**best, "l2_batch": 16}
+    t = measure(over)
+    if t < best_t:
+        best, best_t = over, t
     report = {"key": key, "config": best, "seconds": best_t, "trials": results}
     if use_cache:
         store_cache(key, {"config": best, "seconds": best_t})

@@ -1,0 +1,62 @@
+"""The measuring autotuner: candidate sets and the per-class cache on the CPU;
+on the GPU, that single-solve and batched tuning return configurations that
+solve exactly (tuning changes only the amount of work, never a distance)."""
+import json
+
+import numpy as np
+import pytest
+
+import oracle_lib
+from mlmq_tpds_withl3_b200 import DeviceGraph, HostGraph, Solver, autotune
+
+
+def test_delta_candidates_span_mean_weight_and_default():
+    g = HostGraph.grid(64, 64, seed=3)  # weights U{1000..100000}
+    c = autotune.delta_candidates(g, around=200000)
+    avg = g.info().avg_weight
+    assert c == sorted(c) and 200000 in c
+    assert min(c) == max(1, int(avg * 2)) and all(x <= 800000 for x in c)
+
+
+def test_graph_class_and_cache_roundtrip(tmp_path, monkeypatch):
+    monkeypatch.setenv("MLMQ_TUNE_CACHE", str(tmp_path / "tune.json"))
+    g = HostGraph.rmat(12, seed=5)
+    key = autotune.graph_class(g, "rmat")
+    assert key.startswith("rmat:n2^12:deg")
+    assert autotune.load_cache() == {}
+    autotune.store_cache(key, {"config": {"delta": 5000}, "seconds": 0.01})
+    autotune.store_cache("other", {"config": {}, "seconds": 1.0})
+    data = json.loads((tmp_path / "tune.json").read_text())
+    assert data[key]["config"] == {"delta": 5000} and "other" in data
+
+
+def test_batch_base_settings():
+    b = autotune.BATCH_BASE
+    assert b["l2_batch"] == 16 and b["bucket_max"] == 2 and b["l2_cap_log2"] == 20
+
+
+@pytest.mark.gpu
+def test_tuned_configurations_are_exact(tmp_path, monkeypatch):
+    from mlmq_tpds_withl3_b200 import BatchSolver
+    monkeypatch.setenv("MLMQ_TUNE_CACHE", str(tmp_path / "tune.json"))
+    g = HostGraph.rmat(14, seed=17)
+    dg = DeviceGraph.upload(g)
+    srcs = [0, 1, 2]
+    ref, _ = oracle_lib.sssp_many(g, srcs)
+    cfg, rep = autotune.tune(dg, g, srcs[:2], kind="test-rmat", use_cache=True)
+    assert len(rep["trials"]) >= 10
+    s = Solver(dg, cfg)
+    for k, src in enumerate(srcs):
+        assert np.array_equal(s.solve(src).dist(), ref[k]), (rep["config"], src)
+    # the second call is served from the class cache
+    cfg2, rep2 = autotune.tune(dg, g, srcs[:2], kind="test-rmat", use_cache=True)
+    assert rep2.get("cached") and cfg2.delta == cfg.delta
+    qs = [(dg, x) for x in srcs]
+    cands = [{"delta": 25000, "relax_unroll": 2, "topup": 16},
+             {"delta": 50000, "relax_unroll": 2, "topup": 32, "light_heavy": 1, "bucket_sync": 1}]
+    bcfg, brep = autotune.tune_batch(qs, dg.slots, candidates=cands)
+    assert len(brep["trials"]) == 2 and bcfg.l2_batch == 16 and bcfg.bucket_max == 2
+    b = BatchSolver(len(qs), dg.slots + (dg.n if bcfg.light_heavy else 0), bcfg)
+    b.run(qs)
+    for k in range(len(qs)):
+        assert np.array_equal(b.dist(k), ref[k]), brep["config"]
