@@ -238,7 +238,9 @@ void mlmq_graph_free(mlmq_graph *g);
 int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg, mlmq_solver **out);
 /* Enqueues one complete solve from src on `stream` (a cudaStream_t; NULL =
  * the solver's own stream): distance reset, seed, persistent kernel.
- * Returns after the launch; mlmq_solver_wait reports the outcome. */
+ * Returns after the launch; mlmq_solver_wait reports the outcome.  A launch
+ * while the previous one is outstanding waits for it first (they share the
+ * workspace); the earlier outcome is then not reported. */
 int mlmq_solver_launch(mlmq_solver *s, int src, void *stream);
 /* Blocks until the last launch ends; returns its status as MLMQ_ERR_*. */
 int mlmq_solver_wait(mlmq_solver *s);
@@ -286,7 +288,9 @@ int mlmq_batch_info(const mlmq_batch *b, int *grid, int *block, int *max_queries
 /* Enqueues one launch solving query q from srcs[q] on graphs[q], q < nq.
  * use_graph != 0: the launch (parameter upload, kernel, status download) is
  * captured in a CUDA graph the first time a query set is seen and replayed
- * while the set is unchanged. */
+ * while the set is unchanged.  A run while the previous launch is
+ * outstanding waits for it first (the query table and workspace are
+ * shared); the earlier outcome is then not reported. */
 int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *graphs, const int *srcs,
                    int use_graph, void *stream);
 /* Blocks until the launch ends; the first failing query's MLMQ_ERR_* code. */

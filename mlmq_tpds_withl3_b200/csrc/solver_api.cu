@@ -659,6 +659,15 @@ static int reset_workspace(mlmq_solver *s, cudaStream_t st) {
 extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     if (!s) return MLMQ_ERR_ARG;
     if (src < 0 || src >= s->g->n) return MLMQ_ERR_ARG;
+    // A launch still outstanding (possibly on another stream) uses the same
+    // workspace: it ends first; its status is superseded by this launch's.
+    if (s->launched) {
+        s->launched = false;
+        if (cudaEventSynchronize(s->done) != cudaSuccess) {
+            cudaGetLastError();
+            s->dirty = true;
+        }
+    }
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     int rc = MLMQ_OK;
     if (s->dirty && (rc = reset_workspace(s, st))) return rc;

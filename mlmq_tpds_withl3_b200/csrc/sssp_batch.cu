@@ -267,6 +267,16 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
             return MLMQ_ERR_ARG;
         if (graphs[q]->device != b->device) return MLMQ_ERR_ARG;
     }
+    // A launch still outstanding reads the pinned query table (its copy, or
+    // a graph replay) and writes the workspace: it ends before either is
+    // reused.  Its status is superseded by this launch's.
+    if (b->launched) {
+        b->launched = false;
+        if (cudaEventSynchronize(b->done) != cudaSuccess) {
+            cudaGetLastError();
+            b->dirty = true;
+        }
+    }
     cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
     int rc = MLMQ_OK;
     if (b->dirty && (rc = reset_all(b, st))) return rc;

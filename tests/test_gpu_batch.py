@@ -68,3 +68,28 @@ def test_batch_matches_plain_solver_on_larger_grid():
     for q in (0, 63):
         ref, _ = oracle_lib.sssp_i32(g, srcs[q])
         assert np.array_equal(b.dist(q), ref)
+
+
+def test_back_to_back_launches_without_wait():
+    """A launch while the previous one is outstanding waits for it first:
+    the later query set's results are exact, also through graph replay, and
+    a solver launched twice reports the second source's distances."""
+    from mlmq_tpds_withl3_b200 import Solver
+    import torch
+    g = HostGraph.grid(200, 150, seed=61)
+    dg = DeviceGraph.upload(g)
+    a, b_ = [0, 5, 77], [9000, 12, 29999]
+    ref, _ = oracle_lib.sssp_many(g, a + b_)
+    bs = BatchSolver(4, g.n, {"topup": 32})
+    st = torch.cuda.Stream()
+    for use_graph in (True, False):
+        bs.launch([(dg, s) for s in a], use_graph=use_graph, stream=st.cuda_stream)
+        bs.launch([(dg, s) for s in b_], use_graph=use_graph)
+        bs.wait()
+        for q in range(len(b_)):
+            assert np.array_equal(bs.dist(q), ref[len(a) + q]), (use_graph, q)
+    s = Solver(dg)
+    s.launch(a[1], st.cuda_stream)
+    s.launch(b_[1], None)
+    s.wait()
+    assert np.array_equal(s.dist(), ref[len(a) + 1])
