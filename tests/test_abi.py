@@ -84,3 +84,9 @@ def test_errors_without_device_state():
     assert _lib.lib.sssp_cp_data(ctypes.byref(p)) == _lib.MLMQ_ERR_STATE
     assert _lib.lib.mlmq_solver_launch(None, 0, None) == _lib.MLMQ_ERR_ARG
     assert _lib.lib.mlmq_strerror(-4).decode().startswith("queue ring")
+    # no device memory has been pooled yet: releasing the cache is a no-op
+    assert _lib.lib.mlmq_release_cached() == 0
+    assert _lib.lib.mlmq_graph_prepare_light(None, 100) == _lib.MLMQ_ERR_ARG
+    n = ctypes.c_int()
+    assert _lib.lib.mlmq_server_poll_timed(None, None, None, None, 0,
+                                           ctypes.byref(n)) == _lib.MLMQ_ERR_ARG
