@@ -173,7 +173,8 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
             rec = {"arrival": arr, "start": start, "finish": fin, "latency_s": fin - arr,
                    "solve_ms": solve_ms, "graph": gi, "src": src, "status": status}
             if keep is not None and keep(i):
-                rec["dist"] = buf[:dgraphs[gi].n].numpy().copy()
+                view = buf[:dgraphs[gi].n]  # a torch tensor or a numpy array
+                rec["dist"] = (view.numpy() if hasattr(view, "numpy") else view).copy()
             out[i] = rec
             pool.put(buf)
         if not inflight and pending:
