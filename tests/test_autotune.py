@@ -60,3 +60,53 @@ def test_tuned_configurations_are_exact(tmp_path, monkeypatch):
     b.run(qs)
     for k in range(len(qs)):
         assert np.array_equal(b.dist(k), ref[k]), brep["config"]
+
+
+class _FakeSolver:
+    """Stands in for Solver: remembers the configuration it was built with."""
+
+    def __init__(self, dgraph, cfg):
+        self.cfg = dict(cfg)
+
+    def solve(self, src):
+        return self
+
+    def close(self):
+        pass
+
+
+def _tune_with_cost(monkeypatch, tmp_path, cost):
+    monkeypatch.setenv("MLMQ_TUNE_CACHE", str(tmp_path / "tune.json"))
+    monkeypatch.setattr(autotune, "Solver", _FakeSolver)
+    monkeypatch.setattr(autotune, "_time_solve", lambda s, src, reps=2: cost(s.cfg))
+    g = HostGraph.grid(32, 32, seed=9)
+    return autotune.tune(None, g, [0, 1], kind="fake", use_cache=False)
+
+
+def test_tuner_stages_pick_the_cheapest(monkeypatch, tmp_path):
+    def cost(c):
+        t = abs(c.get("delta", 200000) - 50000) / 1e6 + 1.0
+        t -= 0.1 * (c.get("relax_unroll") == 2) + 0.05 * (c.get("l1_ahead") == 0)
+        return t + 1.0 * bool(c.get("light_heavy")) + 1.0 * (c.get("l2_batch") == 16)
+    cfg, rep = _tune_with_cost(monkeypatch, tmp_path, cost)
+    # the delta stage keeps the candidate nearest 50000; later stages add
+    # their own cheaper settings on top of it
+    best = rep["config"]
+    assert best["relax_unroll"] == 2 and best["l1_ahead"] == 0
+    assert abs(best["delta"] - 50000) == min(abs(d - 50000) for d in
+                                             autotune.delta_candidates(HostGraph.grid(32, 32, seed=9)))
+    assert cfg.relax_unroll == 2 and cfg.l1_ahead == 0
+
+
+def test_tuner_tries_the_split_on_the_default_shape(monkeypatch, tmp_path):
+    """24 warps win without the split, but the split is cheapest with the
+    default shape: the split stage must try that shape too."""
+    def cost(c):
+        if c.get("light_heavy"):
+            return 0.5 if "warps_per_block" not in c else 3.0
+        return 1.0 if c.get("warps_per_block") == 24 else 2.0
+    cfg, rep = _tune_with_cost(monkeypatch, tmp_path, cost)
+    assert rep["config"].get("light_heavy") == 1 and "warps_per_block" not in rep["config"]
+    assert cfg.light_heavy == 1 and cfg.bucket_sync == 1
+    tried = [t["config"] for t in rep["trials"]]
+    assert any(t.get("l2_batch") == 16 for t in tried)
