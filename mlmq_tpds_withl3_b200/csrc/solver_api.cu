@@ -795,6 +795,8 @@ extern "C" int mlmq_release_cached(void) {
 extern "C" int mlmq_solve_host(int n, int64_t m, const int *row, const int *col, const int *w,
                                int nsrc, const int *srcs, int *h_dist, const mlmq_config *cfg) {
     if (nsrc < 0 || (nsrc > 0 && (!srcs || !h_dist))) return MLMQ_ERR_ARG;
+    for (int k = 0; k < nsrc; k++)
+        if (srcs[k] < 0 || srcs[k] >= n) return MLMQ_ERR_ARG;
     mlmq_graph *g = nullptr;
     int rc = mlmq_graph_upload(n, m, row, col, w, &g);
     if (rc) return rc;

@@ -84,6 +84,15 @@ def test_errors_without_device_state():
     assert _lib.lib.sssp_cp_data(ctypes.byref(p)) == _lib.MLMQ_ERR_STATE
     assert _lib.lib.mlmq_solver_launch(None, 0, None) == _lib.MLMQ_ERR_ARG
     assert _lib.lib.mlmq_strerror(-4).decode().startswith("queue ring")
+    # sources are checked before anything touches the device
+    import numpy as np
+    row = np.array([0, 1, 1], np.int32)
+    col = np.array([1], np.int32)
+    w = np.array([5], np.int32)
+    out = np.empty((2, 2), np.int32)
+    srcs = np.array([0, 2], np.int32)
+    assert _lib.lib.mlmq_solve_host(2, 1, row.ctypes.data, col.ctypes.data, w.ctypes.data, 2,
+                                    srcs.ctypes.data, out.ctypes.data, None) == _lib.MLMQ_ERR_ARG
     # no device memory has been pooled yet: releasing the cache is a no-op
     assert _lib.lib.mlmq_release_cached() == 0
     assert _lib.lib.mlmq_graph_prepare_light(None, 100) == _lib.MLMQ_ERR_ARG
