@@ -44,7 +44,8 @@ def test_tuned_configurations_are_exact(tmp_path, monkeypatch):
     srcs = [0, 1, 2]
     ref, _ = oracle_lib.sssp_many(g, srcs)
     cfg, rep = autotune.tune(dg, g, srcs[:2], kind="test-rmat", use_cache=True)
-    assert len(rep["trials"]) >= 10
+    # at least: one delta, two CTA shapes, five single settings, the claim size
+    assert len(rep["trials"]) >= 9
     s = Solver(dg, cfg)
     for k, src in enumerate(srcs):
         assert np.array_equal(s.solve(src).dist(), ref[k]), (rep["config"], src)

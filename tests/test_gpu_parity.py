@@ -238,6 +238,26 @@ def test_l3_one_record_per_vertex_bounds_the_ring():
     assert s.stats()["l3_pushed"] > 0
 
 
+def test_full_l3_ring_is_reported_not_asserted():
+    """Capacity: narrow buckets send almost every record of a 1M-vertex
+    R-MAT graph beyond the window, more distinct vertices than a 2^18-slot
+    L3 ring holds.  A push that finds the ring full waits (bounded) and the
+    solve ends with MLMQ_ERR_QUEUE_FULL -- a status, never a device assert --
+    and the next solve with a fitting ring is exact."""
+    from mlmq_tpds_withl3_b200 import MlmqError
+    from mlmq_tpds_withl3_b200._lib import MLMQ_ERR_QUEUE_FULL, MLMQ_ERR_TIMEOUT
+    g = HostGraph.rmat(20, seed=15)
+    dg = DeviceGraph.upload(g)
+    tight = Solver(dg, {"bucket_num": 2, "bucket_max": 1, "delta": 2000,
+                        "l3_cap_log2": 18, "timeout_ms": 2000})
+    with pytest.raises(MlmqError) as ei:
+        tight.solve(0)
+    assert ei.value.code in (MLMQ_ERR_QUEUE_FULL, MLMQ_ERR_TIMEOUT)
+    tight.close()
+    ref, _ = oracle_lib.sssp_i32(g, 0)
+    assert np.array_equal(Solver(dg).solve(0).dist(), ref)
+
+
 def test_transformed_graphs_solve_exact():
     """G+ (chain shortcuts) and the BFS-reordered graph on the GPU: the same
     distances as the original graph, permuted for the reordering."""
