@@ -377,6 +377,8 @@ void mlmq_server_destroy(mlmq_server *sv);
  *    solve has finished, with its status.
  *  - The first call on a device looks up the workspace address and clears
  *    it; make that first call before any stream capture on that device.
+ *    The set-up belongs to the device's CUDA context: after a
+ *    cudaDeviceReset the next call repeats it.
  *  - All calls share the one workspace and it keeps the last call's
  *    contents: calls whose kernels overlap on the GPU (two host threads,
  *    two streams) race and corrupt each other's results.  Serialise them. */

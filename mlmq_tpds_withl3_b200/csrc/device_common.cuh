@@ -61,6 +61,7 @@ constexpr unsigned ST_DONE = 1u;
 constexpr unsigned ST_TIMEOUT = 2u;
 constexpr unsigned ST_QUEUE_FULL = 4u;
 constexpr unsigned ST_RANGE = 8u;
+constexpr unsigned ST_SLOT_LOST = 16u;  // served query: its slot's CTAs could not meet
 
 // ---- PTX memory-model helpers ------------------------------------------------
 __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {

@@ -26,7 +26,11 @@
 //    other: serialise them;
 //  * the first call on a device looks the workspace's device address up
 //    (cudaGetSymbolAddress, with that device current) and clears it; make
-//    that first call before any stream capture on that device.
+//    that first call before any stream capture on that device.  The set-up
+//    is tied to the device's CUDA context: after a cudaDeviceReset the
+//    library's device image is loaded again (the array comes back
+//    zero-filled, possibly at another address), and the next call repeats
+//    the set-up instead of trusting what it found before.
 #include "mlmq_b200.h"
 #include "solver_internal.h"
 #include "sssp_plain.h"
@@ -61,20 +65,50 @@ __global__ void __launch_bounds__(1024, 1) sssp_noalloc_kernel(PlainParams p) {
 
 struct DeviceSlot {
     unsigned long long *ws = nullptr;  // device address of g_noalloc_ws
+    unsigned long long ctx_id = 0;     // CUDA context the address belongs to (0: unknown)
     bool clean = false;                // every ring slot empty
 };
 std::mutex g_na_mu;
 DeviceSlot g_na_dev[64];
 
-// Once per device, with that device current: resolve the workspace address.
+// The current context's unique id (cuCtxGetId, reached through the runtime's
+// driver entry points so the library needs no link to the driver library),
+// or 0 when it cannot be read.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *a = nullptr, *b = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault) == cudaSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(a);
+            get_id = reinterpret_cast<GetId>(b);
+        }
+        cudaGetLastError();
+        looked_up = true;
+    }
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Once per device context, with that device current: resolve the workspace
+// address.  A context other than the one the address was found in (the
+// device was reset) repeats the set-up and marks the workspace for clearing.
 int workspace_for(int dev, DeviceSlot **out) {
     if (dev < 0 || dev >= 64) return MLMQ_ERR_NODEV;
     DeviceSlot &d = g_na_dev[dev];
-    if (!d.ws) {
+    const unsigned long long ctx = current_context_id();
+    if (!d.ws || ctx == 0 || ctx != d.ctx_id) {
         void *ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_ws);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_ws)");
         d.ws = static_cast<unsigned long long *>(ptr);
+        d.ctx_id = ctx;
         d.clean = false;
     }
     *out = &d;

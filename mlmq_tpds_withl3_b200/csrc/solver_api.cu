@@ -95,6 +95,38 @@ void pinned_ctl_free(unsigned *p) {
     g_pin_free.push_back(p);
 }
 
+namespace {
+// Size classes of the pinned pool: powers of two from 4 KiB.
+std::vector<std::vector<void *>> g_pinned_free(48);
+int pinned_class(size_t bytes) {
+    int c = 12;
+    while (((size_t)1 << c) < bytes) c++;
+    return c;
+}
+}  // namespace
+
+int pinned_alloc(void **p, size_t bytes) {
+    *p = nullptr;
+    const int c = pinned_class(bytes ? bytes : 1);
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto &fl = g_pinned_free[(size_t)c];
+        if (!fl.empty()) {
+            *p = fl.back();
+            fl.pop_back();
+            return MLMQ_OK;
+        }
+    }
+    return cuda_fail(cudaHostAlloc(p, (size_t)1 << c, cudaHostAllocPortable | cudaHostAllocMapped),
+                     "pinned host memory");
+}
+
+void pinned_free(const void *p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pinned_free[(size_t)pinned_class(bytes ? bytes : 1)].push_back(const_cast<void *>(p));
+}
+
 int dev_alloc(void **p, size_t bytes, cudaStream_t st, const char *what) {
     *p = nullptr;
     cudaMemPool_t pool = nullptr;
@@ -243,7 +275,9 @@ int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
         const int blocks = (int)std::min<int64_t>(((int64_t)g->n + 255) / 256, 148 * 16);
         light_split_kernel<<<blocks, 256>>>(g->d_row, g->d_arcs, g->n, delta, d);
         rc = cuda_fail(cudaGetLastError(), "light split launch");
-        if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "light split");
+        // The legacy default stream does not wait for the library's
+        // (non-blocking) solver, batch and server streams.
+        if (!rc) rc = cuda_fail(cudaStreamSynchronize(0), "light split");
     }
     if (rc) {
         dev_free(d, 0);
@@ -401,7 +435,9 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
     g->own_row = false;
     g->d_arcs = nullptr;
     // Everything below is ordered on the legacy default stream; the graph is
-    // complete when this returns (one device synchronisation at the end).
+    // complete when this returns (one synchronisation of that stream at the
+    // end; it does not wait for the library's non-blocking streams, so a
+    // graph can be built while a server kernel runs).
     int rc = cuda_fail(cudaGetDevice(&g->device), "cudaGetDevice");
     if (!rc) rc = dev_alloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1), 0, "alloc(arcs)");
     if (!rc && m > 0) {
@@ -506,8 +542,9 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
         dev_free(d_idx, 0);
         dev_free(d_ht, 0);
     }
-    if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "graph build");
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(0), "graph build");
     if (rc) {
+        cudaStreamSynchronize(0);
         mlmq_graph_free(g);
         return rc;
     }
@@ -571,17 +608,30 @@ extern "C" int mlmq_graph_size(const mlmq_graph *g, int *n, int64_t *m) {
     return MLMQ_OK;
 }
 
-extern "C" void mlmq_graph_free(mlmq_graph *g) {
-    if (!g) return;
-    // Work still reading the graph on any stream ends first (cudaFree's
-    // implicit synchronisation, kept for the pool's stream-ordered frees).
-    cudaDeviceSynchronize();
+namespace mlmq {
+
+void graph_retain(const mlmq_graph *g) {
+    if (g) const_cast<mlmq_graph *>(g)->refs.fetch_add(1, std::memory_order_relaxed);
+}
+
+void graph_release(const mlmq_graph *gc) {
+    if (!gc) return;
+    auto *g = const_cast<mlmq_graph *>(gc);
+    if (g->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+    // Last reference: every solver, batch and served query that read the
+    // graph has ended (each drops its reference only after its work is
+    // done), so the memory goes back to the pool, stream-ordered, without
+    // waiting for unrelated work on the device.
     dev_free(g->d_arcs, 0);
     dev_free(g->d_tiles, 0);
     for (auto &e : g->split_cache) dev_free(e.second, 0);
     if (g->own_row) dev_free(g->d_row, 0);
     delete g;
 }
+
+}  // namespace mlmq
+
+extern "C" void mlmq_graph_free(mlmq_graph *g) { graph_release(g); }
 
 // ---- solver context ----------------------------------------------------------
 
@@ -598,6 +648,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
 
     auto *s = new (std::nothrow) mlmq_solver;
     if (!s) return MLMQ_ERR_NOMEM;
+    graph_retain(g);  // dropped by mlmq_solver_destroy after its last launch
     s->g = g;
     s->cfg = cfg;
     s->device = g->device;
@@ -606,7 +657,7 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
     s->nids = g->slots() + (cfg.light_heavy ? g->n : 0);
     if (cfg.light_heavy && (rc = graph_light_split(g, cfg.delta, &s->split))) {
-        delete s;
+        mlmq_solver_destroy(s);
         return rc;
     }
     s->l3_log = cfg.l3_cap_log2 ? cfg.l3_cap_log2 : l3_ring_log2(s->nids, g->m);
@@ -781,6 +832,7 @@ extern "C" void mlmq_solver_destroy(mlmq_solver *s) {
     pinned_ctl_free(s->h_ctl);
     if (s->done) cudaEventDestroy(s->done);
     if (s->stream) cudaStreamDestroy(s->stream);
+    graph_release(s->g);
     delete s;
 }
 

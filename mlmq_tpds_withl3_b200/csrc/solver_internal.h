@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <utility>
@@ -11,6 +12,12 @@
 #include "mlmq_b200.h"
 
 struct mlmq_graph {
+    // References: the caller's handle (dropped by mlmq_graph_free) plus one
+    // per solver, per batch query set and per served query that reads the
+    // graph.  Its device memory goes back to the pool when the last one is
+    // dropped, after the work that read it has ended -- never by a device-wide
+    // synchronisation, which would wait for a running server kernel.
+    std::atomic<int> refs{1};
     int n = 0;
     int64_t m = 0;
     int device = 0;
@@ -62,6 +69,23 @@ void dev_free(const void *p, cudaStream_t st);
 // One page-locked control-block copy (ctl::WORDS words) from a reused slab.
 int pinned_ctl_alloc(unsigned **p);
 void pinned_ctl_free(unsigned *p);
+// Page-locked, device-mapped host memory from a process-wide pool of size
+// classes.  Blocks go back to the pool, never to the driver: cudaFreeHost,
+// like cudaFree, synchronises the device, and a batch or server freed while
+// another server's persistent kernel runs must not wait for that kernel.
+int pinned_alloc(void **p, size_t bytes);
+template <class T>
+int pinned_alloc(T **p, size_t bytes) {
+    void *v = nullptr;
+    const int rc = pinned_alloc(&v, bytes);
+    *p = static_cast<T *>(v);
+    return rc;
+}
+void pinned_free(const void *p, size_t bytes);
+// Graph references (see mlmq_graph::refs).  graph_release frees the graph
+// when it drops the last reference.
+void graph_retain(const mlmq_graph *g);
+void graph_release(const mlmq_graph *g);
 int fill_device(int *p, int64_t n, int v, cudaStream_t s);
 // Light arcs (weight < delta) of each vertex of g, computed once per delta
 // and kept with the graph.

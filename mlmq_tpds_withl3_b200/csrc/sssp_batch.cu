@@ -109,6 +109,10 @@ struct mlmq_batch {
     cudaGraphExec_t exec = nullptr;   // captured launch of the current query set
     std::vector<long long> exec_key;  // (graph pointer, src) per slot of `exec`
     bool graph_cooperative = true;
+    // Graphs referenced by the last launch and by `exec` (one reference
+    // each): they stay allocated while a launch or a replay may read them,
+    // and a freed graph's address cannot come back as a stale `exec_key`.
+    std::vector<const mlmq_graph *> held;
 };
 
 namespace {
@@ -232,14 +236,16 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     const size_t nq = (size_t)max_queries;
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
     if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_dist, sizeof(int) * nq * (size_t)max_vertices), "batch dist");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l2, sizeof(unsigned long long) * l2_slots(b) * nq), "batch L2");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3, sizeof(unsigned long long) * (nq << b->l3_log)), "batch L3");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_l3bits, sizeof(unsigned) * b->bits_words * nq), "batch L3 bits");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "batch ctl");
-    if (!rc) rc = cuda_fail(cudaMalloc(&b->d_queries, sizeof(BatchQuery) * nq), "batch queries");
-    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_queries, sizeof(BatchQuery) * nq), "pinned queries");
-    if (!rc) rc = cuda_fail(cudaMallocHost(&b->h_ctl, sizeof(unsigned) * CTL_STRIDE * nq), "pinned ctl");
+    // Device memory from the stream-ordered pool and pinned memory from the
+    // pinned pool: destroying a batch then never synchronises the device.
+    if (!rc) rc = dev_alloc(&b->d_dist, sizeof(int) * nq * (size_t)max_vertices, b->stream, "batch dist");
+    if (!rc) rc = dev_alloc(&b->d_l2, sizeof(unsigned long long) * l2_slots(b) * nq, b->stream, "batch L2");
+    if (!rc) rc = dev_alloc(&b->d_l3, sizeof(unsigned long long) * (nq << b->l3_log), b->stream, "batch L3");
+    if (!rc) rc = dev_alloc(&b->d_l3bits, sizeof(unsigned) * b->bits_words * nq, b->stream, "batch L3 bits");
+    if (!rc) rc = dev_alloc(&b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq, b->stream, "batch ctl");
+    if (!rc) rc = dev_alloc(&b->d_queries, sizeof(BatchQuery) * nq, b->stream, "batch queries");
+    if (!rc) rc = pinned_alloc(&b->h_queries, sizeof(BatchQuery) * nq);
+    if (!rc) rc = pinned_alloc(&b->h_ctl, sizeof(unsigned) * CTL_STRIDE * nq);
     if (!rc) rc = reset_all(b, b->stream);
     if (!rc) rc = cuda_fail(cudaStreamSynchronize(b->stream), "batch init");
     if (rc) {
@@ -280,6 +286,12 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
     cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
     int rc = MLMQ_OK;
     if (b->dirty && (rc = reset_all(b, st))) return rc;
+    // No launch of this batch is outstanding now: the graphs of this query
+    // set replace the ones held for the previous one.
+    std::vector<const mlmq_graph *> hold(graphs, graphs + nq);
+    for (const mlmq_graph *g : hold) graph_retain(g);
+    for (const mlmq_graph *g : b->held) graph_release(g);
+    b->held.swap(hold);
     std::vector<long long> key;
     key.reserve(2 * (size_t)nq);
     b->n_of.assign((size_t)nq, 0);
@@ -403,16 +415,20 @@ extern "C" int mlmq_batch_copy_dist(mlmq_batch *b, int q, int *h_dist) {
 
 extern "C" void mlmq_batch_destroy(mlmq_batch *b) {
     if (!b) return;
+    // The last launch may have gone to a caller's stream.
+    if (b->launched && b->done) cudaEventSynchronize(b->done);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    cudaFree(b->d_dist);
-    cudaFree(b->d_l2);
-    cudaFree(b->d_l3);
-    cudaFree(b->d_l3bits);
-    cudaFree(b->d_ctl);
-    cudaFree(b->d_queries);
-    if (b->h_queries) cudaFreeHost(b->h_queries);
-    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    const size_t nq = (size_t)b->max_q;
+    dev_free(b->d_dist, b->stream);
+    dev_free(b->d_l2, b->stream);
+    dev_free(b->d_l3, b->stream);
+    dev_free(b->d_l3bits, b->stream);
+    dev_free(b->d_ctl, b->stream);
+    dev_free(b->d_queries, b->stream);
+    pinned_free(b->h_queries, sizeof(BatchQuery) * nq);
+    pinned_free(b->h_ctl, sizeof(unsigned) * CTL_STRIDE * nq);
+    for (const mlmq_graph *g : b->held) graph_release(g);
     if (b->done) cudaEventDestroy(b->done);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;

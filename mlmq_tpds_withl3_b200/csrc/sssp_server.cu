@@ -20,8 +20,12 @@
 // that copy is done.  Queries on different graphs and of different sizes run
 // side by side; a query's result does not depend on what else runs.
 //
-// Every wait is bounded: by the server's lifetime deadline, by a host-set
-// shutdown flag, and inside a solve by the per-query time limit.
+// Every wait is bounded.  An idle slot waits for its next command until the
+// server's lifetime ends or the host sets the shutdown flag.  Everything a
+// slot does for one query -- the solve and the group barriers around its
+// end -- is bounded by that query's own time limit plus a margin, so a query
+// always gets a completion within that time: a slot whose CTAs cannot all
+// meet reports ST_TIMEOUT | ST_SLOT_LOST and takes no further queries.
 #include "mlmq_b200.h"
 #include "solver_internal.h"
 #include "sssp_plain.h"
@@ -31,6 +35,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -48,8 +53,13 @@ constexpr int SRV_CMD = 456;      // device copy of the command: row, arcs, tile
                                   // bucket_sync, nids, split (2 words)
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
+constexpr int SRV_LOST = 482;     // a CTA of the slot gave up on a group barrier
 constexpr int SRV_BAR_COUNT = 488;
 constexpr int SRV_BAR_GEN = 489;
+// Time the CTAs of a slot may take, past the query's own limit, to meet
+// after a solve (every CTA leaves the solve by that limit); the environment
+// variable MLMQ_SERVER_MEET_MS overrides it at server creation.
+constexpr unsigned long long SRV_MEET_NS = 2000000000ull;
 
 __device__ __forceinline__ unsigned long long ld_acquire64(const volatile unsigned long long *p) {
     unsigned long long v;
@@ -81,6 +91,7 @@ struct alignas(64) SlotCompletion {
     volatile unsigned long long relaxed, pushed;
     // device clock (ns): the slot took the command / reported the result
     volatile unsigned long long t_start, t_end;
+    volatile unsigned lost;  // 1: the slot's CTAs stopped serving (see SRV_LOST)
 };
 
 struct ServerParams {
@@ -97,9 +108,15 @@ struct ServerParams {
     const int *slot_first;        // [slots + 1] first CTA of each slot
     int slots, max_n;
     unsigned long long lifetime_ns;
+    unsigned long long meet_ns;  // how long past a query's limit its CTAs may take to meet
+    int absent_cta;  // test of the bounded barrier: this CTA leaves after its first solve (-1: none)
 };
 
-// Group barrier on words outside the solve's control words.
+// Group barrier on words outside the solve's control words.  A CTA that
+// gives up at `deadline` marks the slot lost (SRV_LOST); a CTA that passes
+// the barrier but finds the mark set fails too, so the CTAs of a slot agree
+// that it is lost unless one gave up after the others had checked -- then
+// the next command finds the mark (see the command wait).
 __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long deadline) {
     __shared__ int ok;
     __syncthreads();
@@ -115,6 +132,7 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
             unsigned ns = 64;
             while (ld_acquire(c + SRV_BAR_GEN) == gen) {
                 if (globaltimer() > deadline) {
+                    atomicOr(c + SRV_LOST, 1u);
                     ok = 0;
                     break;
                 }
@@ -122,6 +140,7 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
                 if (ns < 2048) ns <<= 1;
             }
         }
+        if (ok && ld_acquire(c + SRV_LOST)) ok = 0;
     }
     __syncthreads();
     return ok != 0;
@@ -149,6 +168,16 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
             stop = 0;
             unsigned ns = 256;
             for (;;) {
+                if (ld_acquire(c + SRV_LOST)) {
+                    // A CTA of this slot gave up on a barrier after the last
+                    // completion: the slot can no longer meet; tell the host.
+                    if (grank == 0) {
+                        sp.done[s].lost = 1u;
+                        __threadfence_system();
+                    }
+                    stop = 1;
+                    break;
+                }
                 if (grank == 0) {
                     if (ld_acquire(const_cast<const unsigned *>(sp.shutdown))) {
                         st_release(c + SRV_STOP, 1u);
@@ -209,6 +238,9 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         __syncthreads();
         if (stop) return;
         seen = go_seq;
+        // This CTA's view of when the query started: its solve ends by this
+        // plus the query's time limit.
+        const unsigned long long t_go = globaltimer();
         // ---- one solve --------------------------------------------------------
         PlainParams p = sp.base;
         const volatile unsigned *cmd = c + SRV_CMD;
@@ -231,29 +263,37 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         p.l3bits = sp.l3bits + (size_t)s * sp.bits_words;
         p.ctlw = c;
         plain_body<ArcsInterleaved, K>(p, grank, gsize);
-        // A solve that stopped early leaves records in the rings: the group
-        // empties them before the slot is reused.
+        if ((int)blockIdx.x == sp.absent_cta) return;  // test: a CTA that never arrives
+        // Every CTA of the slot leaves the solve before anything else: after
+        // this barrier nothing writes the status word any more, so every CTA
+        // reads the same final status (read before it, a CTA could miss a
+        // bit that a slower CTA still sets, and the CTAs would then take
+        // different barriers below).  Bounded by the query's own limit.
+        bool ok = group_barrier(c, gsize, t_go + p.timeout_ns + sp.meet_ns);
         __shared__ unsigned solve_status;
         if (threadIdx.x == 0) solve_status = ld_acquire(c + ctl::STATUS);
         __syncthreads();
-        if (solve_status & (ST_TIMEOUT | ST_QUEUE_FULL)) {
-            if (!group_barrier(c, gsize, end)) return;
+        if (ok && (solve_status & (ST_TIMEOUT | ST_QUEUE_FULL))) {
+            // A solve that stopped early leaves records in the rings: the
+            // group empties them before the slot is reused.
             const size_t l2n = (size_t)(p.nb + 1) << p.l2_log, l3n = (size_t)1 << p.l3_log;
             for (size_t i = (size_t)grank * blockDim.x + threadIdx.x; i < l2n + l3n;
                  i += (size_t)gsize * blockDim.x) {
                 if (i < l2n) p.l2[i] = SENT;
                 else p.l3[i - l2n] = SENT;
             }
+            ok = group_barrier(c, gsize, globaltimer() + sp.meet_ns);
         }
-        // Every CTA of the slot has left the solve before it is reported.
-        const bool ok = group_barrier(c, gsize, end);
         if (grank == 0 && threadIdx.x == 0) {
             const unsigned long long *u = reinterpret_cast<const unsigned long long *>(c + ctl::STATS);
-            unsigned st = ld_acquire(c + ctl::STATUS);
+            unsigned st = solve_status;
             // A grid barrier of the solve that gave up left its arrival count
             // behind; no CTA of the slot is inside the solve now.
             if (st & ST_TIMEOUT) st_relaxed(c + ctl::BAR_COUNT, 0u);
-            if (!ok) st |= ST_TIMEOUT;
+            if (!ok) {
+                st |= ST_TIMEOUT | ST_SLOT_LOST;
+                sp.done[s].lost = 1u;
+            }
             sp.done[s].status = st;
             sp.done[s].first_max = (unsigned)u[ctl::ST_FIRST_MAX];
             sp.done[s].relaxed = u[ctl::ST_RELAXED];
@@ -306,6 +346,8 @@ struct mlmq_server {
         unsigned long long seq = 0;     // last command issued
         bool busy = false;              // solving or copying out
         bool copying = false;
+        bool lost = false;              // the slot's CTAs stopped serving
+        const mlmq_graph *g = nullptr;  // graph of the query in the slot (one reference)
         unsigned long long ticket = 0;
         int *h_out = nullptr;
         int n = 0;
@@ -360,6 +402,8 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
                             8 * (((size_t)(cfg.bucket_num + 1) << sv->l2_log) + ((size_t)1 << sv->l3_log)) +
                             4 * SRV_CTL_STRIDE + 4 * sv->bits_words;
     size_t free_b = 0, total_b = 0;
+    // Memory the library's pool keeps for reuse counts as free here.
+    if (!rc) rc = mlmq_release_cached();
     if (!rc) rc = cuda_fail(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
     if (!rc) {
         const size_t reserve = (size_t)2 << 30;
@@ -399,26 +443,30 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
         for (int c = 0; c < sv->slot_ctas[s]; c++) cta_slot.push_back(s);
         slot_first.push_back(slot_first.back() + sv->slot_ctas[s]);
     }
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_cta_slot, sizeof(int) * cta_slot.size()), "server CTA map");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_slot_first, sizeof(int) * slot_first.size()), "server slots");
-    if (!rc) rc = cuda_fail(cudaMemcpy(sv->d_cta_slot, cta_slot.data(), sizeof(int) * cta_slot.size(),
-                                       cudaMemcpyHostToDevice), "H2D CTA map");
-    if (!rc) rc = cuda_fail(cudaMemcpy(sv->d_slot_first, slot_first.data(),
-                                       sizeof(int) * slot_first.size(), cudaMemcpyHostToDevice),
-                            "H2D slots");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_dist, sizeof(int) * ns * (size_t)max_vertices), "server dist");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l2, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log)), "server L2");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3, 8 * (ns << sv->l3_log)), "server L3");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_l3bits, 4 * ns * sv->bits_words), "server L3 bits");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_ctl, 4 * ns * SRV_CTL_STRIDE), "server ctl");
-    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_cmd, sizeof(SlotCommand) * ns, cudaHostAllocDefault), "cmd");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_cmd, sizeof(SlotCommand) * ns), "server mailboxes");
-    if (!rc) rc = cuda_fail(cudaMalloc(&sv->d_shutdown, 64), "server shutdown flag");
-    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_done, sizeof(SlotCompletion) * ns, cudaHostAllocMapped), "done");
-    if (!rc) rc = cuda_fail(cudaHostAlloc(&sv->h_shutdown, 64, cudaHostAllocDefault), "shutdown");
+    // Device memory from the stream-ordered pool, host memory from the
+    // pinned pool: destroying a server never synchronises the device (a
+    // plain cudaFree would wait for every other running kernel).
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking), "kstream");
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "cstream");
     if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&sv->qstream, cudaStreamNonBlocking), "qstream");
+    cudaStream_t ks = sv->kstream;
+    if (!rc) rc = dev_alloc(&sv->d_cta_slot, sizeof(int) * cta_slot.size(), ks, "server CTA map");
+    if (!rc) rc = dev_alloc(&sv->d_slot_first, sizeof(int) * slot_first.size(), ks, "server slots");
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(sv->d_cta_slot, cta_slot.data(), sizeof(int) * cta_slot.size(),
+                                            cudaMemcpyHostToDevice, ks), "H2D CTA map");
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(sv->d_slot_first, slot_first.data(),
+                                            sizeof(int) * slot_first.size(), cudaMemcpyHostToDevice, ks),
+                            "H2D slots");
+    if (!rc) rc = dev_alloc(&sv->d_dist, sizeof(int) * ns * (size_t)max_vertices, ks, "server dist");
+    if (!rc) rc = dev_alloc(&sv->d_l2, 8 * ns * ((size_t)(cfg.bucket_num + 1) << sv->l2_log), ks, "server L2");
+    if (!rc) rc = dev_alloc(&sv->d_l3, 8 * (ns << sv->l3_log), ks, "server L3");
+    if (!rc) rc = dev_alloc(&sv->d_l3bits, 4 * ns * sv->bits_words, ks, "server L3 bits");
+    if (!rc) rc = dev_alloc(&sv->d_ctl, 4 * ns * SRV_CTL_STRIDE, ks, "server ctl");
+    if (!rc) rc = pinned_alloc(&sv->h_cmd, sizeof(SlotCommand) * ns);
+    if (!rc) rc = dev_alloc(&sv->d_cmd, sizeof(SlotCommand) * ns, ks, "server mailboxes");
+    if (!rc) rc = dev_alloc(&sv->d_shutdown, 64, ks, "server shutdown flag");
+    if (!rc) rc = pinned_alloc(&sv->h_done, sizeof(SlotCompletion) * ns);
+    if (!rc) rc = pinned_alloc(&sv->h_shutdown, 64);
     if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&sv->kdone, cudaEventDisableTiming), "kdone");
     if (!rc) {
         std::memset((void *)sv->h_cmd, 0, sizeof(SlotCommand) * ns);
@@ -470,6 +518,12 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
         sp.slots = sv->slots;
         sp.max_n = max_vertices;
         sp.lifetime_ns = (unsigned long long)lifetime_ms * 1000000ull;
+        sp.meet_ns = SRV_MEET_NS;
+        sp.absent_cta = -1;
+        // Test hooks of the bounded slot barrier (tests/test_gpu_server.py).
+        if (const char *e = std::getenv("MLMQ_SERVER_MEET_MS"))
+            if (std::atoi(e) > 0) sp.meet_ns = (unsigned long long)std::atoi(e) * 1000000ull;
+        if (const char *e = std::getenv("MLMQ_SERVER_TEST_ABSENT_CTA")) sp.absent_cta = std::atoi(e);
         if (!rc) {
             cudaLaunchConfig_t lc = {};
             lc.gridDim = dim3((unsigned)sv->grid);
@@ -550,10 +604,13 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     std::lock_guard<std::mutex> lk(sv->mu);
     if (!sv->running) return MLMQ_ERR_STATE;
     int free_slot = -1;
-    for (int s = 0; s < sv->slots; s++)
-        if (!sv->st[s].busy && sv->slot_ctas[s] >= want &&
+    for (int s = 0; s < sv->slots; s++) {
+        auto &c = sv->st[s];
+        if (!c.busy && !c.lost && sv->h_done[s].lost) c.lost = true;
+        if (!c.busy && !c.lost && sv->slot_ctas[s] >= want &&
             (free_slot < 0 || sv->slot_ctas[s] < sv->slot_ctas[free_slot]))
             free_slot = s;
+    }
     if (free_slot < 0) return MLMQ_ERR_BUSY;
     auto &sl = sv->st[free_slot];
     SlotCommand &cmd = sv->h_cmd[free_slot];
@@ -577,6 +634,8 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     sl.ticket = sv->next_ticket++;
     sl.h_out = h_out;
     sl.n = g->n;
+    graph_retain(g);  // dropped when the query's result is reported
+    sl.g = g;
     cmd.seq = sl.seq;
     // Fields first, then the sequence number: in one stream the second copy
     // starts after the first has landed.  The staging entry is not written
@@ -590,6 +649,8 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
                             "command sequence");
     if (rc) {
         sl.busy = false;
+        graph_release(sl.g);
+        sl.g = nullptr;
         return rc;
     }
     *ticket = sl.ticket;
@@ -612,15 +673,33 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
     if (!sv || !count || (max > 0 && (!tickets || !statuses))) return MLMQ_ERR_ARG;
     std::lock_guard<std::mutex> lk(sv->mu);
     int rc = MLMQ_OK;
+    // Whether the server kernel has ended (lifetime, shutdown or an error):
+    // queries it never completed are then reported as failed.
+    const bool ended = sv->running ? cudaEventQuery(sv->kdone) == cudaSuccess : true;
     for (int s = 0; s < sv->slots; s++) {
         auto &sl = sv->st[s];
         if (!sl.busy) continue;
         if (!sl.copying) {
-            if (sv->h_done[s].seq != sl.seq) continue;
+            if (sv->h_done[s].seq != sl.seq) {
+                // No completion: the slot stopped serving (its CTAs could not
+                // meet) or the kernel is gone.  The query fails; its host
+                // buffer was not written.
+                const bool lost = sv->h_done[s].lost != 0;
+                if (lost || ended) {
+                    sl.lost = sl.lost || lost;
+                    sl.busy = false;
+                    graph_release(sl.g);
+                    sl.g = nullptr;
+                    sv->finished.push_back(
+                        {sl.ticket, lost ? MLMQ_ERR_TIMEOUT : MLMQ_ERR_STATE, 0ull});
+                }
+                continue;
+            }
             std::atomic_thread_fence(std::memory_order_acquire);
             sl.status = sv->h_done[s].status;
             sl.relaxed = sv->h_done[s].relaxed;
             sl.solve_ns = sv->h_done[s].t_end - sv->h_done[s].t_start;
+            if (sl.status & ST_SLOT_LOST) sl.lost = true;
             rc = cuda_fail(cudaMemcpyAsync(sl.h_out, sv->d_dist + (size_t)s * sv->max_n,
                                            sizeof(int) * (size_t)sl.n, cudaMemcpyDeviceToHost,
                                            sv->cstream), "server D2H");
@@ -630,6 +709,8 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
         } else if (cudaEventQuery(sl.copied) == cudaSuccess) {
             sl.busy = false;
             sl.copying = false;
+            graph_release(sl.g);
+            sl.g = nullptr;
             sv->finished.push_back({sl.ticket, status_to_error(sl.status), sl.solve_ns});
         }
     }
@@ -643,7 +724,7 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
     }
     *count = k;
     // The server kernel ending early (lifetime or an error) is reported too.
-    if (sv->running && cudaEventQuery(sv->kdone) == cudaSuccess) sv->running = false;
+    if (ended) sv->running = false;
     return MLMQ_OK;
 }
 
@@ -651,7 +732,7 @@ extern "C" int mlmq_server_busy_slots(mlmq_server *sv, int *busy) {
     if (!sv || !busy) return MLMQ_ERR_ARG;
     std::lock_guard<std::mutex> lk(sv->mu);
     int b = 0;
-    for (auto &sl : sv->st) b += sl.busy;
+    for (auto &sl : sv->st) b += sl.busy || sl.lost;
     *busy = b;
     return sv->running ? MLMQ_OK : MLMQ_ERR_STATE;
 }
@@ -676,21 +757,26 @@ extern "C" int mlmq_server_stop(mlmq_server *sv) {
 
 extern "C" void mlmq_server_destroy(mlmq_server *sv) {
     if (!sv) return;
-    mlmq_server_stop(sv);
-    for (auto &sl : sv->st)
+    mlmq_server_stop(sv);  // the kernel has ended and result copies are done
+    for (auto &sl : sv->st) {
         if (sl.copied) cudaEventDestroy(sl.copied);
-    cudaFree(sv->d_dist);
-    cudaFree(sv->d_l2);
-    cudaFree(sv->d_l3);
-    cudaFree(sv->d_l3bits);
-    cudaFree(sv->d_ctl);
-    cudaFree(sv->d_cta_slot);
-    cudaFree(sv->d_slot_first);
-    if (sv->h_cmd) cudaFreeHost(sv->h_cmd);
-    cudaFree(sv->d_cmd);
-    cudaFree(sv->d_shutdown);
-    if (sv->h_done) cudaFreeHost(sv->h_done);
-    if (sv->h_shutdown) cudaFreeHost(sv->h_shutdown);
+        graph_release(sl.g);
+        sl.g = nullptr;
+    }
+    const size_t ns = (size_t)sv->slots;
+    cudaStream_t ks = sv->kstream;
+    dev_free(sv->d_dist, ks);
+    dev_free(sv->d_l2, ks);
+    dev_free(sv->d_l3, ks);
+    dev_free(sv->d_l3bits, ks);
+    dev_free(sv->d_ctl, ks);
+    dev_free(sv->d_cta_slot, ks);
+    dev_free(sv->d_slot_first, ks);
+    dev_free(sv->d_cmd, ks);
+    dev_free(sv->d_shutdown, ks);
+    pinned_free(sv->h_cmd, sizeof(SlotCommand) * ns);
+    pinned_free(sv->h_done, sizeof(SlotCompletion) * ns);
+    pinned_free(sv->h_shutdown, 64);
     if (sv->kdone) cudaEventDestroy(sv->kdone);
     if (sv->kstream) cudaStreamDestroy(sv->kstream);
     if (sv->cstream) cudaStreamDestroy(sv->cstream);

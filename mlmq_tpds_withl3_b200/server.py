@@ -122,11 +122,20 @@ def poisson_schedule(rate, count, graphs_n, seed=1):
     return list(zip(t.tolist(), gi.tolist(), src))
 
 
+HOST_TIMEOUT = "host_timeout"
+
+
 def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0, knobs=None):
     """Runs the schedule against the server.  Returns a list of dicts
     (arrival, start, finish, latency_s, solve_ms, graph, src, status[, dist]) in
     schedule order; `keep(i)` selects the queries whose distances are kept;
-    `knobs[graph index]` (optional) is that graph's per-query Config."""
+    `knobs[graph index]` (optional) is that graph's per-query Config.
+
+    A run that has not finished after `timeout_s` (host clock) stops there:
+    queries still waiting or in flight get status HOST_TIMEOUT (and finish
+    None) instead of an exception, so the caller sees every other query's
+    status.  Queries still in flight keep their pinned buffers: close the
+    server before reusing `pool`."""
     pool = pool or PinnedPool(server.slots, max(g.n for g in dgraphs))
     pending = deque(range(len(schedule)))
     inflight = {}
@@ -135,7 +144,11 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
     while pending or inflight:
         now = time.perf_counter() - t0
         if now > timeout_s:
-            raise TimeoutError("serving did not finish in time")
+            for i, buf, start in list(inflight.values()) + [(i, None, None) for i in pending]:
+                arr, gi, src = schedule[i]
+                out[i] = {"arrival": arr, "start": start, "finish": None, "latency_s": None,
+                          "solve_ms": None, "graph": gi, "src": src, "status": HOST_TIMEOUT}
+            break
         # Admit arrived queries in arrival order while slots and buffers are
         # free; a query whose slot size is all taken is passed over (it keeps
         # its place) so that it does not hold back queries that fit.
@@ -186,26 +199,34 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
 
 def summarize(records, names=None):
     """Throughput, latency percentiles and error counts of a served run;
-    with `names` (graph index -> name) also per graph."""
-    lat = np.array([r["latency_s"] for r in records]) * 1e3
-    span = max(r["finish"] for r in records) - min(r["arrival"] for r in records)
+    with `names` (graph index -> name) also per graph.  Throughput and
+    latency count the queries that finished; every other status (device
+    error codes and HOST_TIMEOUT) is counted in `error_codes`."""
+    done = [r for r in records if r["finish"] is not None]
     codes = {}
     for r in records:
         if r["status"]:
             codes[str(r["status"])] = codes.get(str(r["status"]), 0) + 1
-    out = {"queries": len(records), "qps": len(records) / span,
-           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-           "mean_ms": float(lat.mean()), "errors": sum(codes.values()), "error_codes": codes}
+    out = {"queries": len(records), "finished": len(done), "errors": sum(codes.values()),
+           "error_codes": codes}
+    if done:
+        lat = np.array([r["latency_s"] for r in done]) * 1e3
+        span = max(r["finish"] for r in done) - min(r["arrival"] for r in done)
+        out.update({"qps": len(done) / span, "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean())})
+    else:
+        out.update({"qps": 0.0, "p50_ms": None, "p99_ms": None, "mean_ms": None})
     if names is not None:
         per = {}
         for gi, name in enumerate(names):
-            sel = [r for r in records if r["graph"] == gi]
+            sel = [r for r in done if r["graph"] == gi]
             if not sel:
                 continue
             run = np.array([r["finish"] - r["start"] for r in sel]) * 1e3
             gl = np.array([r["latency_s"] for r in sel]) * 1e3
             per[name] = {"queries": len(sel), "errors": sum(1 for r in sel if r["status"]),
                          "p50_ms": float(np.percentile(gl, 50)),
+                         "p99_ms": float(np.percentile(gl, 99)),
                          "run_ms_mean": float(run.mean()),
                          "solve_ms_mean": float(np.mean([r["solve_ms"] for r in sel]))}
         out["per_graph"] = per

@@ -258,7 +258,10 @@ def test_full_l3_ring_is_reported_not_asserted():
     else:  # had every record fitted after all, the result must be exact
         assert np.array_equal(got, ref)
     tight.close()
-    assert np.array_equal(Solver(dg).solve(0).dist(), ref)
+    after = Solver(dg)
+    assert np.array_equal(after.solve(0).dist(), ref)
+    after.close()
+    dg.close()
 
 
 def test_transformed_graphs_solve_exact():
@@ -286,9 +289,13 @@ def test_timeout_is_reported_not_hung():
     with pytest.raises(MlmqError) as ei:
         s.solve(0)
     assert ei.value.code == MLMQ_ERR_TIMEOUT
+    del ei  # its traceback would keep this frame's solvers alive until a GC pass
     s.close()
     ref, _ = oracle_lib.sssp_i32(g, 0)
-    assert np.array_equal(Solver(dg).solve(0).dist(), ref)
+    after = Solver(dg)
+    assert np.array_equal(after.solve(0).dist(), ref)
+    after.close()
+    dg.close()
 
 
 def test_dropin_entry_points_with_device_csr():

@@ -131,9 +131,34 @@ def test_summary_counts_errors_per_graph():
     assert s["per_graph"]["a"]["solve_ms_mean"] == pytest.approx(0.5)
 
 
-def test_serving_gives_up_after_its_time_limit():
+def test_serving_gives_up_after_its_time_limit_with_statuses():
+    """A query that never completes ends the run at the host time limit;
+    every query gets a record: the one in flight and the one still waiting
+    carry HOST_TIMEOUT, and the summary counts them as errors."""
+    from mlmq_tpds_withl3_b200.server import HOST_TIMEOUT
     graphs = [FakeGraph(4)]
     sv = FakeServer([1], polls=10**9)
-    with pytest.raises(TimeoutError):
-        serve_poisson(sv, graphs, [(0.0, 0, 1), (0.0, 0, 2)], pool=ListPool(2, 4),
-                      timeout_s=0.2)
+    recs = serve_poisson(sv, graphs, [(0.0, 0, 1), (0.0, 0, 2)], pool=ListPool(2, 4),
+                         timeout_s=0.2)
+    assert [r["status"] for r in recs] == [HOST_TIMEOUT, HOST_TIMEOUT]
+    assert recs[0]["start"] is not None and recs[1]["start"] is None
+    s = summarize(recs)
+    assert s["finished"] == 0 and s["errors"] == 2 and s["qps"] == 0.0
+
+
+def test_serving_reports_finished_and_timed_out_queries_together():
+    graphs = [FakeGraph(4)]
+
+    class Stuck(FakeServer):
+        def poll_timed(self):
+            done = super().poll_timed()
+            return [d for d in done if d[0] != 2]  # ticket 2 never completes
+
+    sv = Stuck([1, 1], polls=1)
+    from mlmq_tpds_withl3_b200.server import HOST_TIMEOUT
+    recs = serve_poisson(sv, graphs, [(0.0, 0, k) for k in range(3)], pool=ListPool(3, 4),
+                         timeout_s=0.3)
+    statuses = sorted(str(r["status"]) for r in recs)
+    assert statuses == ["0", "0", HOST_TIMEOUT]
+    s = summarize(recs)
+    assert s["finished"] == 2 and s["errors"] == 1 and s["error_codes"] == {HOST_TIMEOUT: 1}
