@@ -1,38 +1,53 @@
 #!/usr/bin/env python3
-"""Benchmark of the plain single-source delta-stepping solve on B200.
+"""Benchmark of the delta-stepping SSSP path on B200.
 
-Default workload (N=1): the planar road-like kNN graph -- 6.3M points uniform
-in the unit square, 3 nearest neighbours symmetrised, w = round(1e6*d)+1 --
-with 5 seeded sources solved one at a time and delta autotuned around
-200000.  One step = those 5 solves.
+Default run (N=1, ``--workload all``): ONE JSON line whose headline
+``value`` is the plain single-source solve on the planar road-like kNN graph
+(6.3M points uniform in the unit square, 3 nearest neighbours symmetrised,
+w = round(1e6*d)+1, 5 seeded sources solved one at a time, configuration
+tuned on other sources) and which carries three more measured blocks:
+
+  "c3"       plain solves on R-MAT scale 22 (edge factor 16, w U{1..2^20}),
+  "batched"  64 sources on a 4896^2 road-like grid in one persistent launch
+             replayed from a CUDA graph, against 64 back-to-back plain solves,
+  "served"   continuous batching over 8 HBM-resident graphs under Poisson
+             arrivals (1000/s offered, and a saturating burst), p50/p99
+             latency, against back-to-back plain solves of the same mix.
+
+Every result of every block is checked against the CPU oracle outside the
+timed regions: plain and batched distances element by element, served
+results by the device-computed digest of each distance array against the
+digest of the oracle's distances (``correct``).  Each block has its own
+clock record, sampled while its timed work ran.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mlmq|reference]
-                  [--workload c1|c2|c3] [--sources S]
+                  [--workload all|c1|c2|c3|c4|c5] [--skip c3,batched,served]
 
-* value: GTEPS = sum of arcs out of reached vertices (the oracle's
-  total_work) / summed device time of the solves, CUDA events on the launch
-  stream, inputs resident in HBM, L2 flushed (256 MiB write) between solves.
+* value: GTEPS = arcs out of reached vertices (the oracle's total_work) /
+  summed device time of the solves, CUDA events on the launch stream, inputs
+  resident in HBM, L2 flushed (256 MiB write) between solves.
 * e2e: the same metric through mlmq_solve_host() with pinned host buffers:
   CSR upload, every solve, every distance copy back.
 * roofline: algorithmic bytes per solve 12*m_r + 12*n_r over the kernel's
   average duration, against the measured HBM copy bandwidth.
 * cpu_baseline: the reference's own sssp_sequential (oracle/_ref) -- or the
   oracle port when it was not built -- on the host, one thread.
-* --impl reference: the reference's CPU implementation alone, one thread per
-  source, on the same workload and metric.
+* --impl reference: the reference's CPU implementation alone, one host
+  thread per source, on the headline workload and metric.
 
-Multi-GPU (torchrun): replicas only -- every rank solves the same job on its
-own GPU with no collective on the data path; time is the max over ranks.
+Multi-GPU (torchrun): replicas only -- every rank solves the same headline
+job on its own GPU with no collective on the data path; time is the max over
+ranks.  The c3/batched/served blocks are measured at N=1 only.
 """
 import argparse
 import csv
 import io
 import json
 import os
+import platform
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
 
@@ -42,6 +57,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "SSSP GTEPS (plain single-source delta-stepping, queries one at a time)"
+BATCH_METRIC = "SSSP queries/sec (batched: 64 sources in one persistent launch)"
+SERVE_METRIC = "SSSP queries/sec (served: continuous batching over 8 HBM-resident graphs)"
 WORKLOAD_TEXT = {
     "c1": "grid 512x512, 4-neighbour, 10% undirected edges dropped, w U{1000..100000}, "
           "source 0, delta 200000, L1SLF_L2DQ",
@@ -52,45 +69,46 @@ WORKLOAD_TEXT = {
     "c4": "batched: 64 seeded sources on a 4896x4896 grid (10% edges dropped, "
           "w U{1000..100000}) in one persistent launch replayed from a CUDA graph, "
           "64 int32 distance arrays, vs 64 back-to-back plain solves",
+    "c5": "served: grids 2^16..2^24 + R-MAT 18/20/22 resident; Poisson arrivals, graph and "
+          "source uniform per query",
 }
-BATCH_METRIC = "SSSP queries/sec (batched: 64 sources in one persistent launch)"
+# Scaled-down workloads for functional runs of the whole bench (--small).
+SMALL = {"c2_points": 200_000, "c3_scale": 16, "c4_side": 1024, "c5_max_log2": 18,
+         "c5_rmat": (14, 16)}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("mlmq", "reference"), default="mlmq")
-    ap.add_argument("--workload", choices=("c1", "c2", "c3", "c4", "c5"), default="c2")
-    ap.add_argument("--rates", default="10,100,1000,5000", help="served: arrival rates /s")
-    ap.add_argument("--serve-seconds", type=float, default=3.0)
-    ap.add_argument("--max-queries", type=int, default=4000)
+    ap.add_argument("--workload", choices=("all", "c1", "c2", "c3", "c4", "c5"), default="all")
+    ap.add_argument("--skip", default="", help="all: blocks to leave out (c3,batched,served)")
+    ap.add_argument("--small", action="store_true",
+                    help="scaled-down workloads (functional runs of the whole bench)")
+    ap.add_argument("--served-rate", type=float, default=1000.0,
+                    help="served: offered arrival rate of the latency run (queries/s)")
+    ap.add_argument("--served-queries", type=int, default=1000,
+                    help="served: queries in each of the two runs")
+    ap.add_argument("--burst-rate", type=float, default=20000.0,
+                    help="served: arrival rate of the saturating run (queries/s)")
     ap.add_argument("--slots", type=int, default=64)
-    ap.add_argument("--wide-slots", type=int, default=0,
-                    help="served: wide slots for throughput-bound graphs (0: all slots equal; "
-                         "on the 8-graph mix equal slots measured best)")
-    ap.add_argument("--wide-ctas", type=int, default=54, help="served: CTAs of a wide slot")
     ap.add_argument("--slot-warps", type=int, default=8, help="served: worker warps per CTA")
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
     ap.add_argument("--side", type=int, default=0,
                     help="c4: grid side instead of 4896 (small cases for profiler captures)")
+    ap.add_argument("--batch-steps", type=int, default=10, help="batched: timed launches")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--config", default="",
                     help="c1-c3: JSON overrides of the solver configuration, used instead of "
                          "tuning (reproducible profiler runs)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
-def load_workload(name, limit):
-    from mlmq_tpds_withl3_b200 import workloads
-    g, srcs = workloads.WORKLOADS[name]()
-    if limit:
-        srcs = srcs[:limit]
-    return g, srcs
-
+# ---- measurement helpers ----------------------------------------------------------
 
 def measured_peak():
     try:
@@ -149,6 +167,7 @@ class ClockSampler:
         rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 9]
         if not rows:
             return None
+
         def num(x):
             try:
                 return float(x)
@@ -164,19 +183,38 @@ class ClockSampler:
                 "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(args):
+def host_cpu():
+    """Model name and core count of this host (for CPU figures)."""
+    model = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
 
 
+def oracle_lib():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    return ol
+
+
 def cpu_reference_gteps(g, srcs, threads):
     """Times the reference's sssp_sequential (or the oracle port) on the host."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-    fn = oracle_lib.ref_sequential if oracle_lib.reference() is not None else oracle_lib.sssp_i32
-    kind = "reference" if oracle_lib.reference() is not None else "port"
+    ol = oracle_lib()
+    fn = ol.ref_sequential if ol.reference() is not None else ol.sssp_i32
+    kind = "reference" if ol.reference() is not None else "port"
 
     def one(src):
         t0 = time.perf_counter()
@@ -195,63 +233,75 @@ def cpu_reference_gteps(g, srcs, threads):
     return work, wall, busy, kind
 
 
-def run_reference(args):
-    world, rank, _ = dist_setup(args)
-    if rank != 0:
-        return 0
-    g, srcs = load_workload(args.workload, args.sources)
-    threads = max(1, min(len(srcs), os.cpu_count() or 1))
-    for _ in range(args.warmup):
-        cpu_reference_gteps(g, srcs, threads)
-    work = wall = 0.0
-    kind = "reference"
-    for _ in range(args.steps):
-        w, t, _, kind = cpu_reference_gteps(g, srcs, threads)
-        work += w
-        wall += t
-    gteps = work / wall / 1e9
-    line = {
-        "impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_TEXT[args.workload], "n": g.n, "m": g.m,
-                   "sources": srcs},
-        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": kind,
-                         "sample": f"{len(srcs)} sources per step, one host thread each, "
-                                   f"sssp_sequential (SS/SSSP/main.cu:47)"},
-        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-    return 0
+def graph_digest(g):
+    """Fingerprint of a CSR (row, col, w), so both arms can show they ran the
+    same graph."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in (g.row, g.col, g.w):
+        h.update(np.ascontiguousarray(a, dtype=np.int32).tobytes())
+    return h.hexdigest()[:16]
 
 
-def run_mlmq(args):
+def cfg_summary(cfg, keys=("delta", "warps_per_block", "work_blocks", "relax_unroll",
+                           "vertex_tiles", "l1_ahead", "light_heavy", "bucket_sync", "l2_batch",
+                           "topup", "queue_type")):
+    d = {k: getattr(cfg, k) for k in keys}
+    d["queue"] = "L1SLF_L2DQ" if d.pop("queue_type") == 19 else "L1V_L2DQ"
+    return d
+
+
+# ---- workloads -------------------------------------------------------------------
+
+def headline_workload(args):
+    """The headline (C2 unless --workload c1/c3) graph and timed sources."""
+    from mlmq_tpds_withl3_b200 import workloads
+    name = args.workload if args.workload in ("c1", "c2", "c3") else "c2"
+    if name == "c1":
+        g, srcs = workloads.c1()
+    elif name == "c2":
+        g, srcs = workloads.c2(points=SMALL["c2_points"]) if args.small else workloads.c2()
+    else:
+        g, srcs = workloads.c3(scale=SMALL["c3_scale"]) if args.small else workloads.c3()
+    if args.sources:
+        srcs = srcs[:args.sources]
+    return name, g, srcs
+
+
+def workload_config(name, g, srcs, small):
+    """The workload keys of `config`, identical in both arms."""
+    text = WORKLOAD_TEXT[name] + (" [scaled down: --small]" if small else "")
+    return {"workload": text, "n": g.n, "m": g.m, "sources": [int(s) for s in srcs],
+            "graph_sha256_16": graph_digest(g)}
+
+
+# ---- plain single-source arm -------------------------------------------------------
+
+def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_on):
+    """Tuned plain solves of `srcs` on `g`, one at a time.  Returns a dict of
+    JSON fields (value in GTEPS, roofline, e2e, correct, clocks ...)."""
     import torch
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    from mlmq_tpds_withl3_b200.replicas import Replicas, whole_job_rate
-    rep = Replicas("nccl")
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, autotune, default_config
+    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, autotune, default_config, workloads
     from mlmq_tpds_withl3_b200._lib import check, lib
+    from mlmq_tpds_withl3_b200.replicas import whole_job_rate
+    ol = oracle_lib()
+    world = rep.world
 
-    g, srcs = load_workload(args.workload, args.sources)
     dg = DeviceGraph.upload(g)
     tune_report = None
     if args.config:
         cfg = default_config(**{"delta": 200000, **json.loads(args.config)})
-    elif args.workload == "c1" or args.no_tune:
+    elif name == "c1" or args.no_tune:
         cfg = default_config(delta=200000)
     else:
-        cfg, tune_report = autotune.tune(dg, g, srcs[:2], kind=args.workload, use_cache=False)
+        pool = workloads.c3_source_pool(g) if name == "c3" else None
+        probes = workloads.probe_sources(g, srcs, count=4, pool=pool)
+        cfg, tune_report = autotune.tune(dg, g, probes, kind=name, use_cache=False)
     solver = Solver(dg, cfg)
 
-    # Correctness and per-query work (oracle, untimed).
-    dists, works = oracle_lib.sssp_many(g, srcs, threads=min(len(srcs), os.cpu_count() or 1))
-    reached = (dists != oracle_lib.INT_MAX).sum(axis=1)
+    # Correctness and per-query work (oracle, untimed): every timed source.
+    dists, works = ol.sssp_many(g, srcs, threads=min(len(srcs), os.cpu_count() or 1))
+    reached = (dists != ol.INT_MAX).sum(axis=1)
     correct = True
     for k, s in enumerate(srcs):
         solver.solve(s)
@@ -274,7 +324,7 @@ def run_mlmq(args):
             if events is not None:
                 events.append((e0, e1))
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step(None)
     torch.cuda.synchronize()
     rep.barrier()
@@ -282,7 +332,7 @@ def run_mlmq(args):
     sampler = ClockSampler(local)
     with sampler:
         t_wall0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(steps):
             step(events)
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall0
@@ -290,23 +340,25 @@ def run_mlmq(args):
     per_query_ms = np.array([a.elapsed_time(b) for a, b in events])
     total_s = rep.max(per_query_ms.sum() / 1e3)
     work_step = float(np.sum(works))
-    gteps = whole_job_rate(work_step * args.steps, world, total_s) / 1e9
+    gteps = whole_job_rate(work_step * steps, world, total_s) / 1e9
 
     # Roofline of the persistent kernel.
     bytes_q = 12.0 * np.asarray(works, np.float64) + 12.0 * reached.astype(np.float64)
     launch_s = per_query_ms / 1e3
-    achieved_gbs = float(np.sum(np.tile(bytes_q, args.steps)) / np.sum(launch_s) / 1e9)
+    achieved_gbs = float(np.sum(np.tile(bytes_q, steps)) / np.sum(launch_s) / 1e9)
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic("sssp_plain_kernel", args.workload)
+    traffic = ncu_traffic("sssp_plain_kernel", name)
+    stats = solver.stats()
+    solver.close()
 
     # End to end through the host-buffer API.
     e2e = None
-    if not args.no_e2e:
+    if e2e_on:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
         row, col, w = pin(g.row), pin(g.col), pin(g.w)
         src_arr = np.asarray(srcs, np.int32)
         out = torch.empty((len(srcs), g.n), dtype=torch.int32).pin_memory()
-        e2e_steps = max(1, min(args.steps, 5))
+        e2e_steps = max(1, min(steps, 5))
         walls = []
         for i in range(e2e_steps + 1):
             t0 = time.perf_counter()
@@ -317,39 +369,35 @@ def run_mlmq(args):
                 walls.append(time.perf_counter() - t0)
         e2e_s = rep.max(float(np.sum(walls)))
         correct = correct and np.array_equal(out.numpy(), dists)
-        e2e = {"value": whole_job_rate(work_step * len(walls), world, e2e_s) / 1e9, "unit": "GTEPS",
+        e2e = {"value": whole_job_rate(work_step * len(walls), world, e2e_s) / 1e9,
+               "unit": "GTEPS",
                "h2d_bytes_per_step": int(4 * (g.n + 1) + 8 * g.m),
                "d2h_bytes_per_step": int(4 * g.n * len(srcs)),
                "ms_per_step": e2e_s / len(walls) * 1e3,
                "walls_ms": [round(x * 1e3, 2) for x in walls],
                "api": "mlmq_solve_host (pinned host CSR in, distances out)"}
+        del out, row, col, w
     del dists
+    dg.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        work, wall, busy, kind = cpu_reference_gteps(g, srcs, 1)
+    if cpu_baseline and rep.rank == 0 and world == 1:
+        work, wall, _, kind = cpu_reference_gteps(g, srcs, 1)
         cpu = {"value": work / wall / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+               "host_cpu": host_cpu(),
                "sample": f"{len(srcs)} sources of the same workload, one after another, "
                          f"{wall:.1f} s"}
 
-    rep.close()
-    if rank != 0:
-        return 0
-    clocks = sampler.summary()
-    line = {
-        "metric": METRIC, "value": gteps, "unit": "GTEPS", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded generator; the reference's DIMACS graphs are not available)",
-        "config": {"workload": WORKLOAD_TEXT[args.workload], "n": g.n, "m": g.m,
-                   "sources": srcs, "queue": "L1SLF_L2DQ" if cfg.queue_type == 19 else "L1V_L2DQ",
-                   "delta": cfg.delta, "warps_per_block": cfg.warps_per_block,
-                   "work_blocks": solver.stats()["grid"],
-                   "l2_between_solves": "flushed (256 MiB write, outside the timed events)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+    out = {
+        "value": gteps, "unit": "GTEPS", "steps": steps, "warmup": warmup,
+        "ms_per_step": total_s / steps * 1e3,
+        "config": workload_config(name, g, srcs, args.small),
+        "solver": {**cfg_summary(cfg), "grid": stats["grid"], "block": stats["block"],
+                   "l2_between_solves": "flushed (256 MiB write, outside the timed events)"},
         "correct": bool(correct),
-        "qps": whole_job_rate(len(srcs) * args.steps, world, total_s),
+        "checked": f"every timed source ({len(srcs)}) element by element against the oracle, "
+                   f"device-resident and through mlmq_solve_host",
+        "qps": whole_job_rate(len(srcs) * steps, world, total_s),
         "latency_ms": {"p50": float(np.percentile(per_query_ms, 50)),
                        "p99": float(np.percentile(per_query_ms, 99))},
         "work_per_step": int(work_step),
@@ -358,59 +406,59 @@ def run_mlmq(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel": "sssp_plain_kernel",
                      "algorithmic_bytes_per_launch": float(np.mean(bytes_q))},
-        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary(),
         "gpu_launches": len(events), "wall_s_timed_region": t_wall,
+        "relax_per_arc": float(stats["relaxed"]) / max(1.0, float(works[-1])),
     }
     if tune_report:
-        line["autotune"] = {"config": tune_report.get("config"),
-                            "trials": len(tune_report.get("trials", []))}
-    print(json.dumps(line), flush=True)
-    return 0
+        out["autotune"] = {"config": tune_report.get("config"),
+                           "probe_sources": tune_report.get("probe"),
+                           "trials": len(tune_report.get("trials", []))}
+    return out
 
 
-def run_batched(args):
+# ---- batched arm (C4) ----------------------------------------------------------------
+
+BATCH_CANDIDATES = (
+    [{"delta": d, "relax_unroll": 2, "topup": 32} for d in (25000, 50000, 100000)]
+    + [{"delta": 25000, "relax_unroll": 2, "topup": 16},
+       {"delta": 50000, "relax_unroll": 4, "topup": 16}]
+    + [{"delta": d, "relax_unroll": 2, "topup": 32, "light_heavy": 1, "bucket_sync": 1}
+       for d in (25000, 50000)])
+
+
+def batched_arm(args, rep, local):
     """C4: one step = one batched launch of all sources (CUDA-graph replay)."""
     import torch
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    from mlmq_tpds_withl3_b200.replicas import Replicas, whole_job_rate
-    rep = Replicas("nccl")
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-    from mlmq_tpds_withl3_b200 import BatchSolver, DeviceGraph, Solver, default_config
-
+    from mlmq_tpds_withl3_b200 import BatchSolver, DeviceGraph, Solver, autotune, default_config
     from mlmq_tpds_withl3_b200 import workloads
-    g, srcs = workloads.c4(side=args.side) if args.side else workloads.c4()
+    from mlmq_tpds_withl3_b200.replicas import whole_job_rate
+    ol = oracle_lib()
+    side = args.side or (SMALL["c4_side"] if args.small else 4896)
+    g, srcs = workloads.c4(side=side)
     if args.sources:
         srcs = srcs[:args.sources]
     dg = DeviceGraph.upload(g)
     queries = [(dg, s) for s in srcs]
     tune_report = None
     if args.no_tune:
-        # the configuration the batch tuner settles on for grids
         bcfg = default_config(delta=25000, warps_per_block=8, relax_unroll=2, topup=32,
                               l2_cap_log2=20, l2_batch=16, bucket_max=2)
     else:
-        from mlmq_tpds_withl3_b200 import autotune
-        bcfg, tune_report = autotune.tune_batch(queries, dg.slots)
+        bcfg, tune_report = autotune.tune_batch(queries, dg.slots, candidates=BATCH_CANDIDATES)
     batch = BatchSolver(len(srcs), dg.slots + (dg.n if bcfg.light_heavy else 0), bcfg)
     stream = torch.cuda.Stream()
 
-    # Correctness: oracle on a few sources, the plain solver on every source.
-    check_q = list(range(0, len(srcs), max(1, len(srcs) // 4)))[:4]
-    ref, works_chk = oracle_lib.sssp_many(g, [srcs[q] for q in check_q])
-    batch.run(queries, use_graph=True)
-    correct = all(np.array_equal(batch.dist(q), ref[i]) for i, q in enumerate(check_q))
-    del ref
-    # The back-to-back baseline gets its own tuned single-solve configuration.
+    # The back-to-back baseline gets its own tuned single-solve configuration,
+    # picked on sources other than the timed ones.
     if args.no_tune:
         pcfg = default_config(delta=200000)
     else:
-        from mlmq_tpds_withl3_b200 import autotune
-        pcfg, _ = autotune.tune(dg, g, srcs[:2], kind="c4-plain", use_cache=False)
+        probes = workloads.probe_sources(g, srcs, count=4, pool=np.arange(g.n))
+        pcfg, _ = autotune.tune(dg, g, probes, kind="c4-plain", use_cache=False)
     plain = Solver(dg, pcfg)
-    plain_ms, works, reached = [], [], []
-    for q, s in enumerate(srcs):
+    plain_ms, plain_out = [], []
+    for s in srcs:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -419,13 +467,8 @@ def run_batched(args):
         plain.wait()
         e1.synchronize()
         plain_ms.append(e0.elapsed_time(e1))
-        d = plain.dist()
-        correct = correct and np.array_equal(d, batch.dist(q))
-        fin = d != oracle_lib.INT_MAX
-        reached.append(int(fin.sum()))
-        works.append(int(np.diff(g.row)[fin].sum()))
+        plain_out.append(plain.dist())
     plain.close()
-    work_step = float(sum(works))
 
     for _ in range(args.warmup):
         batch.launch(queries, use_graph=True, stream=stream.cuda_stream)
@@ -433,9 +476,10 @@ def run_batched(args):
     torch.cuda.synchronize()
     rep.barrier()
     events = []
+    steps = max(1, args.batch_steps)
     sampler = ClockSampler(local)
     with sampler:
-        for _ in range(args.steps):
+        for _ in range(steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -447,31 +491,43 @@ def run_batched(args):
     rep.barrier()
     step_ms = np.array([a.elapsed_time(b) for a, b in events])
     total_s = rep.max(step_ms.sum() / 1e3)
-    qps = whole_job_rate(len(srcs) * args.steps, world, total_s)
-    plain_qps = whole_job_rate(len(srcs), world, rep.max(np.sum(plain_ms) / 1e3))
-    rep.close()
+
+    # Every query of the last launch and every back-to-back solve against the
+    # oracle, element by element (outside the timed region).
+    t0 = time.perf_counter()
+    ref, works = ol.sssp_many(g, srcs)
+    correct = True
+    reached = []
+    for q in range(len(srcs)):
+        d = batch.dist(q)
+        correct = correct and np.array_equal(d, ref[q]) and np.array_equal(plain_out[q], ref[q])
+        reached.append(int((ref[q] != ol.INT_MAX).sum()))
+    check_s = time.perf_counter() - t0
+    del ref, plain_out
+    batch.close()
+    dg.close()
+
+    qps = whole_job_rate(len(srcs) * steps, rep.world, total_s)
+    plain_qps = whole_job_rate(len(srcs), rep.world, rep.max(np.sum(plain_ms) / 1e3))
+    work_step = float(np.sum(works))
     bytes_step = 12.0 * work_step + 12.0 * float(sum(reached))
-    achieved = bytes_step * args.steps / total_s / 1e9
+    achieved = bytes_step * steps / total_s / 1e9
     peak, peak_kind = measured_peak()
-    line = {
-        "metric": BATCH_METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD_TEXT["c4"] if not args.side else
-                   f"batched: {len(srcs)} sources on a {args.side}x{args.side} grid (profiling case)",
+    out = {
+        "metric": BATCH_METRIC, "value": qps, "unit": "queries/s", "steps": steps,
+        "warmup": args.warmup, "ms_per_step": total_s / steps * 1e3,
+        "config": {"workload": WORKLOAD_TEXT["c4"] if side == 4896 else
+                   f"batched: {len(srcs)} sources on a {side}x{side} grid (scaled down)",
                    "n": g.n, "m": g.m, "sources": len(srcs),
-                   "delta": bcfg.delta, "warps_per_block": bcfg.warps_per_block,
-                   "l1_ahead": bcfg.l1_ahead, "relax_unroll": bcfg.relax_unroll,
-                   "grid": batch.grid,
-                   "cuda_graph": True, "l2": "inputs (6.1 GB distances, 0.7 GB arcs) exceed L2"},
+                   "graph_sha256_16": graph_digest(g),
+                   "l2": "inputs (6.1 GB distances, 0.7 GB arcs) exceed L2"},
+        "solver": {**cfg_summary(bcfg), "grid": batch.grid, "cuda_graph": True},
         "correct": bool(correct),
-        "gteps": work_step * args.steps / total_s / 1e9,
+        "checked": f"all {len(srcs)} batched results and all {len(srcs)} back-to-back results "
+                   f"element by element against the oracle ({check_s:.1f} s, untimed)",
+        "gteps": work_step * steps / total_s / 1e9,
         "plain_back_to_back": {"qps": plain_qps, "ms_per_query_p50": float(np.median(plain_ms)),
-                               "config": {"delta": pcfg.delta, "warps_per_block": pcfg.warps_per_block,
-                                          "relax_unroll": pcfg.relax_unroll,
-                                          "l1_ahead": pcfg.l1_ahead,
-                                          "vertex_tiles": pcfg.vertex_tiles},
+                               "config": cfg_summary(pcfg),
                                "gteps": work_step / (np.sum(plain_ms) / 1e3) / 1e9},
         "speedup_vs_plain_qps": qps / plain_qps,
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
@@ -485,116 +541,93 @@ def run_batched(args):
         "clocks": sampler.summary(), "gpu_launches": len(events),
     }
     if tune_report:
-        line["autotune"] = {"config": tune_report["config"], "trials": len(tune_report["trials"])}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+        out["autotune"] = {"config": tune_report["config"], "trials": len(tune_report["trials"])}
+    return out
 
 
-SERVE_METRIC = "SSSP queries/sec (served: continuous batching over 8 HBM-resident graphs)"
+# ---- served arm (C5) -----------------------------------------------------------------
+
+SERVE_CANDIDATES = (
+    [{"delta": d, "topup": 32} for d in (25000, 50000, 100000, 200000)]
+    + [{"delta": 50000, "topup": 16}]
+    + [{"delta": d, "topup": 32, "light_heavy": 1, "bucket_sync": 1} for d in (25000, 50000)])
 
 
-def run_served(args):
-    """C5: Poisson arrivals over 8 resident graphs, rate swept 10..5000/s."""
+def served_arm(args, rep, local):
+    """C5: Poisson arrivals over 8 resident graphs: a run at the offered rate
+    (latency) and a saturating burst (throughput); every result's device
+    digest against the oracle's."""
     import torch
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    from mlmq_tpds_withl3_b200.replicas import Replicas
-    rep = Replicas("nccl", timeout_s=1800)
-    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, default_config, workloads
-    from mlmq_tpds_withl3_b200.server import (PinnedPool, Server, poisson_schedule,
-                                              serve_poisson, summarize)
-    hgs = workloads.c5_graphs()
+    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver, autotune, default_config, workloads
+    from mlmq_tpds_withl3_b200._lib import dist_digest
+    from mlmq_tpds_withl3_b200.server import (HOST_TIMEOUT, PinnedPool, Server,
+                                              poisson_schedule, serve_poisson, summarize)
+    ol = oracle_lib()
+    if args.small:
+        hgs = workloads.c5_graphs(max_log2=SMALL["c5_max_log2"], rmat_scales=SMALL["c5_rmat"])
+    else:
+        hgs = workloads.c5_graphs()
     names = list(hgs)
     dgs = [DeviceGraph.upload(hgs[k]) for k in names]
     ns = [hgs[k].n for k in names]
     max_n = max(dg.slots for dg in dgs)
-    tune_report = None
     cfg = default_config(delta=100000, warps_per_block=args.slot_warps, relax_unroll=2,
                          l2_cap_log2=20, l2_batch=16, bucket_max=2)
     knobs = None
-    layout = None
-    grid_max = 3 * 148  # CTAs of 8+1 warps that fit a B200 (the server checks)
-    if args.wide_slots > 0:
-        small = (grid_max - args.wide_slots * args.wide_ctas) // 6
-        layout = [6] * small + [args.wide_ctas] * args.wide_slots
+    tune_report = None
     if not args.no_tune:
-        # Each resident graph gets the per-query settings (delta, topup,
-        # run-ahead bound) that were fastest on a batched launch of 64 of its
-        # own queries in small slots, and is sent to a wide slot when 8 of its
-        # queries in wide slots give more queries/s than that (a
-        # throughput-bound query gains nothing from sharing the GPU in small
-        # pieces).  The server passes the settings with every query.
-        from mlmq_tpds_withl3_b200 import autotune
-        cands = [{"delta": d, "topup": t} for d in (25000, 50000, 100000, 200000)
-                 for t in (16, 32)]
-        cands += [{"delta": 400000, "topup": 16}, {"delta": 200000, "topup": 16, "l1_ahead": 0}]
-        cands += [{"delta": d, "topup": 32, "light_heavy": 1, "bucket_sync": 1}
-                  for d in (25000, 50000, 100000)]
+        # Each resident graph gets the per-query settings that were fastest on
+        # a batched launch of 64 of its own queries (sources other than the
+        # served ones); the server passes them with every query.
         knobs, tune_report = [], {}
         base = {**autotune.BATCH_BASE, "warps_per_block": args.slot_warps, "relax_unroll": 2}
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
-            kc, trep = autotune.tune_batch(qs, dg.slots, candidates=cands, base=base)
-            entry = dict(trep["config"])
-            if layout is not None:
-                qps_small = len(qs) / trep["seconds"]
-                kw, repw = autotune.tune_batch(
-                    qs[:8], dg.slots, candidates=cands,
-                    base={**base, "work_blocks": 8 * args.wide_ctas})
-                qps_wide = 8 / repw["seconds"]
-                entry["qps_small_slots"] = qps_small
-                entry["qps_wide_slots"] = qps_wide
-                if qps_wide > qps_small:
-                    kc = default_config(**{**base, **repw["config"], "work_blocks": args.wide_ctas})
-                    entry = {**repw["config"], "work_blocks": args.wide_ctas,
-                             "qps_small_slots": qps_small, "qps_wide_slots": qps_wide}
+            kc, trep = autotune.tune_batch(qs, dg.slots, candidates=SERVE_CANDIDATES, base=base)
             knobs.append(kc)
-            tune_report[names[i]] = entry
-    if knobs is not None and any(k.light_heavy for k in knobs):
-        max_n = max(max_n, max(dg.slots + dg.n for dg, k in zip(dgs, knobs) if k.light_heavy))
-        for dg, k in zip(dgs, knobs):
-            if k.light_heavy:
-                dg.prepare_light(k.delta)
-    sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900, layout=layout)
+            tune_report[names[i]] = dict(trep["config"])
+        if any(k.light_heavy for k in knobs):
+            max_n = max(max_n, max(dg.slots + dg.n for dg, k in zip(dgs, knobs)
+                                   if k.light_heavy))
+            for dg, k in zip(dgs, knobs):
+                if k.light_heavy:
+                    dg.prepare_light(k.delta)
+    sv = Server(slots=args.slots, max_vertices=max_n, cfg=cfg, lifetime_s=900)
     pool = PinnedPool(sv.slots, max(ns))  # result buffers hold real vertices only
-    rates = [float(r) for r in args.rates.split(",")]
-    sweep = []
-    sample = {}
-    for ri, rate in enumerate(rates):
-        count = int(min(max(30, rate * args.serve_seconds), args.max_queries))
-        sched = poisson_schedule(rate, count, ns, seed=100 + ri)
-        # A kept result is copied out of its pinned buffer inside the serving
-        # loop (up to 67 MB); eight per rate keep that host work small.
-        every = max(1, count // 8)
-        keep = (lambda i, every=every: i % every == 0)
-        recs = serve_poisson(sv, dgs, sched, keep=keep, pool=pool, timeout_s=600, knobs=knobs)
-        s = summarize(recs, names)
-        s["rate"] = rate
-        sweep.append(s)
-        for i, r in enumerate(recs):
-            if "dist" in r:
-                sample[(ri, i)] = r
+    runs = {}
+    scheds = {}
+    sampler = ClockSampler(local)
+    with sampler:
+        for key, rate, seed in (("offered", args.served_rate, 101),
+                                ("saturation", args.burst_rate, 102)):
+            sched = poisson_schedule(rate, args.served_queries, ns, seed=seed)
+            recs = serve_poisson(sv, dgs, sched, pool=pool, timeout_s=600, knobs=knobs)
+            runs[key] = recs
+            scheds[key] = sched
+    clocks = sampler.summary()
+    info = {"slots": sv.slots, "grid": sv.grid, "block": sv.block}
     sv.close()
     del pool
-    # Alone vs in the mix, and back-to-back plain solves of the same mix.
+
+    # Back-to-back plain solves of a sample of the same mix, each graph with
+    # its own tuned single-solve configuration; the same queries alone must
+    # give the digest they had in the mix.
+    sample = runs["saturation"][:96]
     solvers = {}
-    correct = True
-    plain_ms = []
-    plain_by_graph = {}
+    plain_ms, plain_by_graph = [], {}
+    alone_same = True
     stream = torch.cuda.Stream()
-    for (ri, i), r in sample.items():
+    for r in sample:
         gi = r["graph"]
         if gi not in solvers:
-            # Each graph's back-to-back baseline runs its own tuned
-            # single-solve configuration.
             pc = default_config(delta=200000)
             if not args.no_tune:
-                from mlmq_tpds_withl3_b200 import autotune
                 hg = hgs[names[gi]]
-                probe = [int(x) for x in np.random.default_rng(gi).integers(0, hg.n, 2)]
-                pc, _ = autotune.tune(dgs[gi], hg, probe, kind=f"c5-{names[gi]}", use_cache=False)
+                served_srcs = [x["src"] for x in sample if x["graph"] == gi]
+                probe = workloads.probe_sources(hg, served_srcs, count=4, pool=np.arange(hg.n))
+                pc, _ = autotune.tune(dgs[gi], hg, probe, kind=f"c5-{names[gi]}",
+                                      use_cache=False)
             solvers[gi] = Solver(dgs[gi], pc)
         s = solvers[gi]
         e0 = torch.cuda.Event(enable_timing=True)
@@ -606,42 +639,173 @@ def run_served(args):
         e1.synchronize()
         plain_ms.append(e0.elapsed_time(e1))
         plain_by_graph.setdefault(names[gi], []).append(plain_ms[-1])
-        if r["status"] or not np.array_equal(s.dist(), r["dist"]):
-            correct = False
+        if r["status"] != 0 or dist_digest(s.dist()) != r["digest"]:
+            alone_same = False
     for s in solvers.values():
         s.close()
+    for dg in dgs:
+        dg.close()
+
+    # Every served result against the oracle: digest of the oracle's
+    # distances for each (graph, source) served.
+    t0 = time.perf_counter()
+    want = {}
+    for gi, name in enumerate(names):
+        srcs = sorted({r["src"] for recs in runs.values() for r in recs if r["graph"] == gi})
+        if not srcs:
+            continue
+        dgst, _, _ = ol.sssp_digest_many(hgs[name], srcs)
+        for s, d in zip(srcs, dgst):
+            want[(gi, s)] = int(d)
+    check_s = time.perf_counter() - t0
+    bad = 0
+    total = 0
+    for recs in runs.values():
+        for r in recs:
+            total += 1
+            if r["status"] != 0 or r["digest"] != want[(r["graph"], r["src"])]:
+                bad += 1
+    sat = summarize(runs["saturation"], names)
+    off = summarize(runs["offered"], names)
     plain_qps = 1e3 / float(np.mean(plain_ms))
-    top = max(sweep, key=lambda s: s["qps"])
-    # replicas serve independent arrival streams: the whole job's rate is the
-    # sum of theirs (one sum per collective, same order on every rank)
-    top_qps = rep.sum(top["qps"])
+    qps = rep.sum(sat["qps"])
     plain_qps = rep.sum(plain_qps)
-    rep.close()
-    line = {
-        "metric": SERVE_METRIC, "value": top_qps, "unit": "queries/s", "n_gpus": world,
-        "steps": len(rates), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded generators)",
-        "config": {"workload": "served: grids 2^16..2^24 + R-MAT 18/20/22 resident; Poisson "
-                               "arrivals, graph and source uniform per query",
+    out = {
+        "metric": SERVE_METRIC, "value": qps, "unit": "queries/s",
+        "config": {"workload": WORKLOAD_TEXT["c5"] + (" [scaled down]" if args.small else ""),
                    "graphs": {k: {"n": hgs[k].n, "m": hgs[k].m} for k in names},
-                   "slots": sv.slots, "grid": sv.grid, "delta": cfg.delta,
-                   "slot_ctas": sorted(set(sv.layout)) if layout else None,
-                   "wide_slots": args.wide_slots if layout else 0,
-                   "warps_per_block": cfg.warps_per_block, "relax_unroll": cfg.relax_unroll,
-                   "l1_ahead": cfg.l1_ahead, "rates": rates},
-        "sweep": sweep,
-        "latency_ms": {"p50": top["p50_ms"], "p99": top["p99_ms"], "at_rate": top["rate"]},
+                   "queries_per_run": args.served_queries,
+                   "offered_rate": args.served_rate, "burst_rate": args.burst_rate,
+                   **info, "slot_settings": cfg_summary(cfg)},
+        "saturation": {k: sat.get(k) for k in ("qps", "p50_ms", "p99_ms", "mean_ms", "finished",
+                                               "errors", "error_codes")},
+        "offered": {k: off.get(k) for k in ("qps", "p50_ms", "p99_ms", "mean_ms", "finished",
+                                            "errors", "error_codes")},
+        "latency_ms": {"p50": off["p50_ms"], "p99": off["p99_ms"],
+                       "at_offered_rate": args.served_rate},
+        "per_graph_saturation": sat.get("per_graph"),
         "plain_back_to_back": {"qps": plain_qps, "queries": len(plain_ms),
                                "ms_per_query_mean": float(np.mean(plain_ms)),
                                "ms_mean_by_graph": {k: float(np.mean(v))
                                                     for k, v in sorted(plain_by_graph.items())}},
-        "speedup_vs_plain_qps": top_qps / plain_qps,
-        "correct": bool(correct),
-        "checked_alone_vs_mix": len(sample),
+        "speedup_vs_plain_qps": qps / plain_qps,
+        "correct": bool(bad == 0 and alone_same),
+        "checked": f"all {total} served results: status 0 and the device digest of each "
+                   f"distance array equal to the digest of the oracle's distances "
+                   f"({check_s:.1f} s, untimed); {len(sample)} of them also solved alone "
+                   f"with the plain solver, same digest",
+        "mismatches": bad, "alone_equals_mix": bool(alone_same),
+        "clocks": clocks,
     }
     if tune_report:
-        line["autotune"] = {"per_graph_query_settings": tune_report}
+        out["autotune"] = {"per_graph_query_settings": tune_report}
+    del HOST_TIMEOUT
+    return out
+
+
+# ---- arms ------------------------------------------------------------------------------
+
+def run_reference(args):
+    """The reference's own sssp_sequential on the headline workload, one host
+    thread per source; rank 0 only."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    name, g, srcs = headline_workload(args)
+    threads = max(1, min(len(srcs), os.cpu_count() or 1))
+    for _ in range(args.warmup):
+        cpu_reference_gteps(g, srcs, threads)
+    work = wall = 0.0
+    kind = "reference"
+    for _ in range(args.steps):
+        w, t, _, kind = cpu_reference_gteps(g, srcs, threads)
+        work += w
+        wall += t
+    gteps = work / wall / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator; the reference's DIMACS graphs are not available)",
+        "config": workload_config(name, g, srcs, args.small),
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": kind,
+                         "host_cpu": host_cpu(),
+                         "sample": f"{len(srcs)} sources per step, one host thread each, "
+                                   f"sssp_sequential (SS/SSSP/main.cu:47)"},
+        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_mlmq(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from mlmq_tpds_withl3_b200.replicas import Replicas
+    from mlmq_tpds_withl3_b200._lib import lib
+    rep = Replicas("nccl", timeout_s=1800)
+    name, g, srcs = headline_workload(args)
+    res = plain_arm(args, name, g, srcs, rep, local, args.steps, args.warmup,
+                    cpu_baseline=not args.no_cpu_baseline, e2e_on=not args.no_e2e)
+    del g
+    lib.mlmq_release_cached()
+    line = {"metric": METRIC, "value": res.pop("value"), "unit": res.pop("unit"),
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res.pop("ms_per_step"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator; the reference's DIMACS graphs are not available)",
+            "config": res.pop("config"), "parallelism": "replicas" if world > 1 else "single GPU"}
+    res.pop("steps")
+    res.pop("warmup")
+    line.update(res)
+    skip = {s.strip() for s in args.skip.split(",") if s.strip()}
+    if args.workload == "all" and world == 1:
+        blocks_t0 = time.perf_counter()
+        if "c3" not in skip:
+            from mlmq_tpds_withl3_b200 import workloads
+            if args.small:
+                g3, s3 = workloads.c3(scale=SMALL["c3_scale"])
+            else:
+                g3, s3 = workloads.c3()
+            c3 = plain_arm(args, "c3", g3, s3, rep, local, min(args.steps, 10), args.warmup,
+                           cpu_baseline=False, e2e_on=not args.no_e2e)
+            c3["metric"] = "SSSP GTEPS (plain single-source, R-MAT scale 22)"
+            line["c3"] = c3
+            del g3
+            lib.mlmq_release_cached()
+        if "batched" not in skip:
+            line["batched"] = batched_arm(args, rep, local)
+            lib.mlmq_release_cached()
+        if "served" not in skip:
+            line["served"] = served_arm(args, rep, local)
+            lib.mlmq_release_cached()
+        line["blocks_wall_s"] = time.perf_counter() - blocks_t0
+        line["correct_all"] = bool(line["correct"] and all(
+            line[k]["correct"] for k in ("c3", "batched", "served") if k in line))
+    rep.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_single_block(args, which):
+    """--workload c4 or c5: that block alone as the JSON line."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from mlmq_tpds_withl3_b200.replicas import Replicas
+    rep = Replicas("nccl", timeout_s=1800)
+    res = batched_arm(args, rep, local) if which == "c4" else served_arm(args, rep, local)
+    rep.close()
+    line = {"metric": res.pop("metric"), "value": res.pop("value"), "unit": res.pop("unit"),
+            "n_gpus": world, "steps": res.pop("steps", 1), "warmup": res.pop("warmup", 0),
+            "ms_per_step": res.pop("ms_per_step", None), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generators)"}
+    line.update(res)
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -651,10 +815,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "c4":
-        return run_batched(args)
-    if args.workload == "c5":
-        return run_served(args)
+    if args.workload in ("c4", "c5"):
+        return run_single_block(args, args.workload)
     return run_mlmq(args)
 
 

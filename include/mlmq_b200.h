@@ -351,6 +351,26 @@ int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuses, int max,
  * host-side queueing and result copy-out); solve_ns may be NULL. */
 int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *statuses,
                            uint64_t *solve_ns, int max, int *count);
+/* One finished served query. */
+typedef struct mlmq_served_result {
+    uint64_t ticket;
+    int status;        /* MLMQ_ERR_* */
+    uint64_t solve_ns; /* device time, as mlmq_server_poll_timed */
+    uint64_t digest;   /* fingerprint of the distances the slot produced,
+                          computed on the device (mlmq_dist_digest's
+                          definition); 0 when the query failed */
+} mlmq_served_result;
+/* As mlmq_server_poll_timed, with each query's result digest: a caller can
+ * check every served result against a reference digest without keeping the
+ * distance arrays. */
+int mlmq_server_poll_results(mlmq_server *sv, mlmq_served_result *out, int max, int *count);
+/* Digest of a host distance array: the sum, modulo 2^64, of
+ * mix64((v << 32) | (uint32_t)dist[v]) over v < n, mix64 being the
+ * SplitMix64 output function.  Equal arrays give equal digests; a sum of
+ * per-vertex terms, so the device computes it in any order. */
+uint64_t mlmq_dist_digest(const int *dist, int64_t n);
+/* Slots that are busy or out of service; MLMQ_ERR_STATE once the server
+ * kernel has ended. */
 int mlmq_server_busy_slots(mlmq_server *sv, int *busy);
 int mlmq_server_stop(mlmq_server *sv);
 void mlmq_server_destroy(mlmq_server *sv);

@@ -152,6 +152,14 @@ _sig("mlmq_server_poll", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_in
      ctypes.POINTER(c_int))
 _sig("mlmq_server_poll_timed", c_int, c_vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_int),
      ctypes.POINTER(c_u64), c_int, ctypes.POINTER(c_int))
+class ServedResult(ctypes.Structure):
+    """struct mlmq_served_result."""
+    _fields_ = [("ticket", c_u64), ("status", c_int), ("solve_ns", c_u64), ("digest", c_u64)]
+
+
+_sig("mlmq_server_poll_results", c_int, c_vp, ctypes.POINTER(ServedResult), c_int,
+     ctypes.POINTER(c_int))
+_sig("mlmq_dist_digest", c_u64, c_vp, c_i64)
 _sig("mlmq_server_busy_slots", c_int, c_vp, ctypes.POINTER(c_int))
 _sig("mlmq_server_stop", c_int, c_vp)
 _sig("mlmq_server_destroy", None, c_vp)
@@ -160,6 +168,14 @@ _sig("mlmq_sssp_solve_noalloc", c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, c_
      ctypes.POINTER(Config), c_vp)
 NOALLOC_MAX_VERTICES = 1 << 20
 NOALLOC_MAX_ARCS = 1 << 20
+
+
+def dist_digest(dist):
+    """mlmq_dist_digest of an int32 host array (numpy or a CPU torch tensor)."""
+    import numpy as np
+    a = dist.numpy() if hasattr(dist, "numpy") else dist
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return int(lib.mlmq_dist_digest(a.ctypes.data, len(a)))
 
 
 def default_config(**overrides):

@@ -128,6 +128,22 @@ __device__ __forceinline__ unsigned rec_d(unsigned long long r) {
     return (unsigned)(r >> 32) & 0x7fffffffu;
 }
 
+// ---- result digest ---------------------------------------------------------
+// A 64-bit fingerprint of a distance array: the sum, modulo 2^64, of
+// mix64((v << 32) | dist[v]) over every vertex v, where mix64 is the
+// SplitMix64 output function (Steele, Lea and Flood, 2014).  A sum of
+// per-vertex terms, so any split of the vertices over threads gives the same
+// value; mlmq_dist_digest computes it on the host.
+__host__ __device__ __forceinline__ unsigned long long digest_mix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__host__ __device__ __forceinline__ unsigned long long digest_term(unsigned long long v, int d) {
+    return digest_mix64((v << 32) | (unsigned)d);
+}
+
 // ---- grid barrier (the launch is cooperative, so every CTA is resident) ----
 // Returns false when the wait ran past `deadline` (status gets ST_TIMEOUT).
 __device__ __forceinline__ bool grid_barrier(unsigned *ctlw, unsigned nblocks,

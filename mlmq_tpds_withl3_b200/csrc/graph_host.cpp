@@ -571,112 +571,215 @@ int mlmq_hgraph_reorder_bfs(const mlmq_host_graph *g, int root, mlmq_host_graph 
     return MLMQ_OK;
 }
 
-// Chain-shortcut augmentation G+ (reference SSSP/l3/l3_chain_shortcuts.h:
-// 23-109, strict variant).  A vertex is a chain vertex when it is not the
-// source, has exactly two out-arcs to two distinct other vertices on its own
-// side of `cut`, and exactly two in-arcs, which come from those same two
-// vertices.  From every other vertex, each out-arc is followed through chain
-// vertices to the first non-chain vertex; when that walk passes at least one
-// chain vertex, does not return to its start and its weight sum stays below
-// INT_MAX, one shortcut arc (start -> end, summed weight) is added before the
-// vertex's original arcs.  Every original arc is kept, so shortest-path
-// distances are unchanged.  stats (optional, 5 entries): chain vertices,
-// shortcuts, longest walk in arcs, walks dropped for overflow, arcs replaced.
+// Chain-shortcut augmentation G+.  The graph it produces is the one the
+// reference's builder produces (SSSP/l3/l3_chain_shortcuts.h:23-109, strict
+// variant): the same chain vertices, the same shortcut arcs in the same
+// order, the same statistics -- tests compare both byte for byte.  The way
+// it gets there is data-parallel:
+//
+//  1. Chain vertices, one independent test per vertex: not the source,
+//     exactly two out-arcs to two distinct other vertices on its own side of
+//     `cut`, in-degree exactly two, and an arc back from each of its two
+//     out-neighbours (so its two in-arcs come from exactly those vertices).
+//  2. Walks through chains by pointer jumping.  A "step" is an out-arc of a
+//     chain vertex: (c, k) = the k-th out-arc of c, to y.  When y is a chain
+//     vertex the walk continues on y's out-arc that does not return to c;
+//     otherwise the step ends the walk.  Every step starts with its own arc
+//     (weight, one hop, end y) and a link to its successor; each round,
+//     every step adds its successor's totals and links to the successor's
+//     successor, so after ceil(log2 L) rounds every step knows the weight,
+//     hop count and end of the rest of its walk (Wyllie's list ranking).
+//     Steps on a closed ring of chain vertices never finish; no walk from a
+//     non-chain vertex can enter such a ring.
+//  3. From every non-chain vertex u, out-arc f to a chain vertex c continues
+//     on c's step away from u: weight w(f) + the step's total, hops 1 + its
+//     hops.  One shortcut u -> end per such walk that does not come back to
+//     u and whose weight stays below INT_MAX, placed before u's original arcs
+//     in the order of u's out-arcs.  Every original arc is kept, so
+//     shortest-path distances are unchanged.
+//
+// stats (optional, 5 entries): chain vertices, shortcuts, longest walk in
+// arcs, walks dropped for overflow, arcs the shortcuts stand for.
 int mlmq_hgraph_chain_shortcuts(const mlmq_host_graph *g, int cut, int source,
                                 mlmq_host_graph **out, int64_t *stats) {
     if (!g || !out) return MLMQ_ERR_ARG;
     const int n = g->n;
-    const int64_t m = g->m;
     if (source < 0 || source >= n || cut < 0 || cut > n) return MLMQ_ERR_ARG;
     auto *r = new (std::nothrow) mlmq_host_graph;
     if (!r) return MLMQ_ERR_NOMEM;
     int rc = MLMQ_OK;
     try {
         const int *row = g->row.data(), *dst = g->col.data(), *wt = g->w.data();
-        std::vector<unsigned char> chain((size_t)n, 0);
-        std::vector<int> incoming((size_t)n, 0), rev0((size_t)n, -1), rev1((size_t)n, -1);
-        for (int u = 0; u < n; u++) {
-            if (u == source || row[u + 1] - row[u] != 2) continue;
-            const int a = dst[row[u]], b = dst[row[u] + 1];
-            chain[u] = a != u && b != u && a != b && (a < cut) == (u < cut) && (b < cut) == (u < cut);
-        }
-        for (int u = 0; u < n; u++)
-            for (int e = row[u]; e < row[u + 1]; e++) {
-                const int v = dst[e];
-                if (!chain[v]) continue;
-                ++incoming[v];
-                if (u == dst[row[v]]) rev0[v] = e;
-                if (u == dst[row[v] + 1]) rev1[v] = e;
+        // ---- 1. chain vertices ------------------------------------------------
+        std::vector<std::atomic<int>> indeg((size_t)n);
+        parallel_for(n, [&](int64_t b, int64_t e, int) {
+            for (int64_t v = b; v < e; v++) indeg[v].store(0, std::memory_order_relaxed);
+        });
+        parallel_for(g->m, [&](int64_t b, int64_t e, int) {
+            for (int64_t a = b; a < e; a++) indeg[dst[a]].fetch_add(1, std::memory_order_relaxed);
+        });
+        auto has_arc = [&](int from, int to) {
+            for (int a = row[from]; a < row[from + 1]; a++)
+                if (dst[a] == to) return true;
+            return false;
+        };
+        std::vector<int> chain_id((size_t)n, -1);  // compact index of each chain vertex
+        std::vector<unsigned char> is_chain((size_t)n, 0);
+        parallel_for(n, [&](int64_t b, int64_t e, int) {
+            for (int64_t vv = b; vv < e; vv++) {
+                const int v = (int)vv;
+                if (v == source || row[v + 1] - row[v] != 2 || indeg[v].load() != 2) continue;
+                const int x = dst[row[v]], y = dst[row[v] + 1];
+                const bool side = v < cut;
+                if (x == v || y == v || x == y || (x < cut) != side || (y < cut) != side) continue;
+                is_chain[v] = has_arc(x, v) && has_arc(y, v);
             }
-        int64_t nchain = 0, nshort = 0, longest = 0, overflow = 0, replaced = 0;
-        for (int u = 0; u < n; u++) {
-            chain[u] = chain[u] && incoming[u] == 2 && rev0[u] >= 0 && rev1[u] >= 0;
-            nchain += chain[u];
-        }
-        r->n = n;
-        r->row.assign((size_t)n + 1, 0);
-        r->col.reserve((size_t)m);
-        r->w.reserve((size_t)m);
-        for (int u = 0; u < n && !rc; u++) {
-            if (!chain[u])
-                for (int first = row[u]; first < row[u + 1]; first++) {
-                    int prev = u, cur = dst[first];
-                    int64_t hops = 1, cost = wt[first];
-                    bool over = false;
-                    while (chain[cur]) {
-                        int e = row[cur];
-                        if (dst[e] == prev) ++e;
-                        else if (dst[e + 1] != prev) {
-                            rc = MLMQ_ERR_ARG;  // cannot happen for a valid chain vertex
-                            break;
-                        }
-                        cost += wt[e];
-                        ++hops;
-                        prev = cur;
-                        cur = dst[e];
-                        if (cost >= INT_MAX) {
-                            over = true;
-                            break;
-                        }
-                        if (hops > n) {
-                            rc = MLMQ_ERR_ARG;
-                            break;
-                        }
-                    }
-                    if (rc) break;
-                    if (over) {
-                        ++overflow;
+        });
+        int nchain = 0;
+        for (int v = 0; v < n; v++)
+            if (is_chain[v]) chain_id[v] = nchain++;
+        // ---- 2. pointer jumping over chain steps ------------------------------
+        // Step 2*chain_id[c] + k is c's k-th out-arc.
+        const int64_t steps = 2 * (int64_t)nchain;
+        std::vector<int64_t> len((size_t)steps), len2((size_t)steps);
+        std::vector<int> hop((size_t)steps), hop2((size_t)steps);
+        std::vector<int> end((size_t)steps), end2((size_t)steps);
+        std::vector<int> nxt((size_t)steps), nxt2((size_t)steps);
+        // The step of chain vertex c that leaves along the arc not going to `from`.
+        auto away_from = [&](int c, int from) -> int64_t {
+            return 2 * (int64_t)chain_id[c] + (dst[row[c]] == from ? 1 : 0);
+        };
+        parallel_for(n, [&](int64_t b, int64_t e, int) {
+            for (int64_t cc = b; cc < e; cc++) {
+                const int c = (int)cc;
+                if (!is_chain[c]) continue;
+                for (int k = 0; k < 2; k++) {
+                    const int64_t s = 2 * (int64_t)chain_id[c] + k;
+                    const int a = row[c] + k, y = dst[a];
+                    len[s] = wt[a];
+                    hop[s] = 1;
+                    end[s] = y;
+                    nxt[s] = is_chain[y] ? (int)away_from(y, c) : -1;
+                }
+            }
+        });
+        int rounds = 1;
+        while (((int64_t)1 << rounds) <= steps) rounds++;
+        for (int it = 0; it <= rounds; it++) {
+            std::atomic<bool> live(false);
+            parallel_for(steps, [&](int64_t b, int64_t e, int) {
+                bool any = false;
+                for (int64_t s = b; s < e; s++) {
+                    const int t = nxt[s];
+                    if (t < 0) {
+                        len2[s] = len[s];
+                        hop2[s] = hop[s];
+                        end2[s] = end[s];
+                        nxt2[s] = -1;
                         continue;
                     }
-                    if (hops <= 1 || cur == u) continue;
-                    if ((cur < cut) != (u < cut)) {
-                        rc = MLMQ_ERR_ARG;
-                        break;
-                    }
-                    if ((int64_t)r->col.size() >= INT_MAX) {
-                        rc = MLMQ_ERR_RANGE;
-                        break;
-                    }
-                    r->col.push_back(cur);
-                    r->w.push_back((int)cost);
-                    ++nshort;
-                    replaced += hops;
-                    longest = std::max(longest, hops);
+                    // Weights are below 2^31 and a walk has fewer than 2^31
+                    // arcs, so the sum fits in 63 bits.
+                    len2[s] = len[s] + len[t];
+                    hop2[s] = hop[s] + hop[t];
+                    end2[s] = end[t];
+                    nxt2[s] = nxt[t];
+                    any = any || nxt[t] >= 0;
                 }
-            for (int e = row[u]; e < row[u + 1]; e++) {
-                r->col.push_back(dst[e]);
-                r->w.push_back(wt[e]);
-            }
-            if ((int64_t)r->col.size() >= INT_MAX) rc = MLMQ_ERR_RANGE;
-            r->row[u + 1] = (int)r->col.size();
+                if (any) live.store(true);
+            });
+            len.swap(len2);
+            hop.swap(hop2);
+            end.swap(end2);
+            nxt.swap(nxt2);
+            if (!live.load()) break;
         }
-        r->m = (int64_t)r->col.size();
-        if (stats) {
-            stats[0] = nchain;
-            stats[1] = nshort;
-            stats[2] = longest;
-            stats[3] = overflow;
-            stats[4] = replaced;
+        // ---- 3. shortcuts from non-chain vertices -----------------------------
+        // Per out-arc of a non-chain vertex: 0 no shortcut, 1 shortcut,
+        // 2 dropped for overflow.
+        std::vector<unsigned char> kind((size_t)g->m, 0);
+        std::vector<int> count((size_t)n + 1, 0);
+        std::atomic<int> bad(0);
+        parallel_for(n, [&](int64_t b, int64_t e, int) {
+            for (int64_t uu = b; uu < e; uu++) {
+                const int u = (int)uu;
+                int c = row[u + 1] - row[u];
+                if (!is_chain[u])
+                    for (int f = row[u]; f < row[u + 1]; f++) {
+                        const int h = dst[f];
+                        if (!is_chain[h]) continue;
+                        const int64_t s = away_from(h, u);
+                        if (nxt[s] >= 0) {  // cannot happen: walks from u end
+                            bad.store(1);
+                            continue;
+                        }
+                        if ((int64_t)wt[f] + len[s] >= INT_MAX) {
+                            kind[f] = 2;
+                            continue;
+                        }
+                        if (end[s] == u) continue;
+                        if ((end[s] < cut) != (u < cut)) bad.store(1);
+                        kind[f] = 1;
+                        c++;
+                    }
+                count[u + 1] = c;
+            }
+        });
+        if (bad.load()) rc = MLMQ_ERR_ARG;
+        int64_t total = 0;
+        for (int u = 0; u < n && !rc; u++) {
+            total += count[u + 1];
+            if (total >= INT_MAX) rc = MLMQ_ERR_RANGE;
+        }
+        if (!rc) {
+            r->n = n;
+            r->m = total;
+            r->row.assign((size_t)n + 1, 0);
+            for (int u = 0; u < n; u++) r->row[u + 1] = r->row[u] + count[u + 1];
+            r->col.resize((size_t)total);
+            r->w.resize((size_t)total);
+            std::vector<int64_t> part(4 * (size_t)num_threads() + 4, 0);  // per thread: shortcuts,
+                                                                       // longest, overflow, arcs
+            parallel_for(n, [&](int64_t b, int64_t e, int t) {
+                int64_t ns = 0, lg = 0, ov = 0, ar = 0;
+                for (int64_t uu = b; uu < e; uu++) {
+                    const int u = (int)uu;
+                    int p = r->row[u];
+                    for (int f = row[u]; f < row[u + 1]; f++) {
+                        if (kind[f] == 2) ov++;
+                        if (kind[f] != 1) continue;
+                        const int64_t s = away_from(dst[f], u);
+                        r->col[p] = end[s];
+                        r->w[p++] = (int)(wt[f] + len[s]);
+                        const int64_t hops = 1 + (int64_t)hop[s];
+                        ns++;
+                        ar += hops;
+                        lg = std::max(lg, hops);
+                    }
+                    for (int f = row[u]; f < row[u + 1]; f++) {
+                        r->col[p] = dst[f];
+                        r->w[p++] = wt[f];
+                    }
+                }
+                part[4 * (size_t)t] = ns;
+                part[4 * (size_t)t + 1] = lg;
+                part[4 * (size_t)t + 2] = ov;
+                part[4 * (size_t)t + 3] = ar;
+            });
+            if (stats) {
+                int64_t ns = 0, lg = 0, ov = 0, ar = 0;
+                for (size_t t = 0; t + 3 < part.size(); t += 4) {
+                    ns += part[t];
+                    lg = std::max(lg, part[t + 1]);
+                    ov += part[t + 2];
+                    ar += part[t + 3];
+                }
+                stats[0] = nchain;
+                stats[1] = ns;
+                stats[2] = lg;
+                stats[3] = ov;
+                stats[4] = ar;
+            }
         }
     } catch (...) {
         rc = MLMQ_ERR_NOMEM;

@@ -54,6 +54,7 @@ constexpr int SRV_CMD = 456;      // device copy of the command: row, arcs, tile
 constexpr int SRV_GO = 480;       // published command sequence (device)
 constexpr int SRV_STOP = 481;     // shutdown seen by the slot leader
 constexpr int SRV_LOST = 482;     // a CTA of the slot gave up on a group barrier
+constexpr int SRV_DIGEST = 484;   // u64: digest of the slot's last result (8-byte aligned)
 constexpr int SRV_BAR_COUNT = 488;
 constexpr int SRV_BAR_GEN = 489;
 // Time the CTAs of a slot may take, past the query's own limit, to meet
@@ -92,6 +93,7 @@ struct alignas(64) SlotCompletion {
     // device clock (ns): the slot took the command / reported the result
     volatile unsigned long long t_start, t_end;
     volatile unsigned lost;  // 1: the slot's CTAs stopped serving (see SRV_LOST)
+    volatile unsigned long long digest;  // digest_term sum over the result's vertices
 };
 
 struct ServerParams {
@@ -211,6 +213,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                         const unsigned long long spl = (unsigned long long)cm.split;
                         c[SRV_CMD + 15] = (unsigned)spl;
                         c[SRV_CMD + 16] = (unsigned)(spl >> 32);
+                        *reinterpret_cast<unsigned long long *>(c + SRV_DIGEST) = 0ull;
                         __threadfence();
                         // publish the sequence number (low 32 bits) to the group
                         st_release(c + SRV_GO, (unsigned)q);
@@ -282,6 +285,24 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                 if (i < l2n) p.l2[i] = SENT;
                 else p.l3[i - l2n] = SENT;
             }
+        }
+        if (ok) {
+            // Digest of the result, one pass over the distances by the whole
+            // group; the host compares it with a reference digest without
+            // holding every result (mlmq_server_poll_results).
+            __shared__ unsigned long long cta_sum;
+            if (threadIdx.x == 0) cta_sum = 0ull;
+            __syncthreads();
+            unsigned long long part = 0ull;
+            for (size_t i = (size_t)grank * blockDim.x + threadIdx.x; i < (size_t)p.n;
+                 i += (size_t)gsize * blockDim.x)
+                part += digest_term(i, __ldcg(p.dist + i));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
+            if ((threadIdx.x & 31) == 0) atomicAdd(&cta_sum, part);
+            __syncthreads();
+            if (threadIdx.x == 0)
+                atomicAdd(reinterpret_cast<unsigned long long *>(c + SRV_DIGEST), cta_sum);
             ok = group_barrier(c, gsize, globaltimer() + sp.meet_ns);
         }
         if (grank == 0 && threadIdx.x == 0) {
@@ -295,6 +316,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
                 sp.done[s].lost = 1u;
             }
             sp.done[s].status = st;
+            sp.done[s].digest = ld_relaxed64(reinterpret_cast<const unsigned long long *>(c + SRV_DIGEST));
             sp.done[s].first_max = (unsigned)u[ctl::ST_FIRST_MAX];
             sp.done[s].relaxed = u[ctl::ST_RELAXED];
             sp.done[s].pushed = u[ctl::ST_PUSHED];
@@ -355,6 +377,7 @@ struct mlmq_server {
         unsigned status = 0;
         unsigned long long relaxed = 0;
         unsigned long long solve_ns = 0;
+        unsigned long long digest = 0;
     };
     std::vector<Slot> st;
     unsigned long long next_ticket = 1;
@@ -362,6 +385,7 @@ struct mlmq_server {
         unsigned long long ticket;
         int status;
         unsigned long long solve_ns;  // device time from command pickup to result
+        unsigned long long digest;    // device digest of the distances (0 when none)
     };
     std::deque<Finished> finished;
 };
@@ -668,9 +692,12 @@ extern "C" int mlmq_server_poll(mlmq_server *sv, uint64_t *tickets, int *statuse
     return mlmq_server_poll_timed(sv, tickets, statuses, nullptr, max, count);
 }
 
-extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *statuses,
-                                      uint64_t *solve_ns, int max, int *count) {
-    if (!sv || !count || (max > 0 && (!tickets || !statuses))) return MLMQ_ERR_ARG;
+namespace {
+
+// Advances the slots (see mlmq_server_poll_timed) and reports up to `max`
+// finished queries through `emit(index, finished)`.
+template <class Emit>
+int server_poll(mlmq_server *sv, int max, int *count, Emit emit) {
     std::lock_guard<std::mutex> lk(sv->mu);
     int rc = MLMQ_OK;
     // Whether the server kernel has ended (lifetime, shutdown or an error):
@@ -691,7 +718,7 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
                     graph_release(sl.g);
                     sl.g = nullptr;
                     sv->finished.push_back(
-                        {sl.ticket, lost ? MLMQ_ERR_TIMEOUT : MLMQ_ERR_STATE, 0ull});
+                        {sl.ticket, lost ? MLMQ_ERR_TIMEOUT : MLMQ_ERR_STATE, 0ull, 0ull});
                 }
                 continue;
             }
@@ -699,6 +726,7 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
             sl.status = sv->h_done[s].status;
             sl.relaxed = sv->h_done[s].relaxed;
             sl.solve_ns = sv->h_done[s].t_end - sv->h_done[s].t_start;
+            sl.digest = sv->h_done[s].digest;
             if (sl.status & ST_SLOT_LOST) sl.lost = true;
             rc = cuda_fail(cudaMemcpyAsync(sl.h_out, sv->d_dist + (size_t)s * sv->max_n,
                                            sizeof(int) * (size_t)sl.n, cudaMemcpyDeviceToHost,
@@ -711,14 +739,12 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
             sl.copying = false;
             graph_release(sl.g);
             sl.g = nullptr;
-            sv->finished.push_back({sl.ticket, status_to_error(sl.status), sl.solve_ns});
+            sv->finished.push_back({sl.ticket, status_to_error(sl.status), sl.solve_ns, sl.digest});
         }
     }
     int k = 0;
     while (k < max && !sv->finished.empty()) {
-        tickets[k] = sv->finished.front().ticket;
-        statuses[k] = sv->finished.front().status;
-        if (solve_ns) solve_ns[k] = sv->finished.front().solve_ns;
+        emit(k, sv->finished.front());
         sv->finished.pop_front();
         k++;
     }
@@ -726,6 +752,36 @@ extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *s
     // The server kernel ending early (lifetime or an error) is reported too.
     if (ended) sv->running = false;
     return MLMQ_OK;
+}
+
+}  // namespace
+
+extern "C" int mlmq_server_poll_timed(mlmq_server *sv, uint64_t *tickets, int *statuses,
+                                      uint64_t *solve_ns, int max, int *count) {
+    if (!sv || !count || (max > 0 && (!tickets || !statuses))) return MLMQ_ERR_ARG;
+    return server_poll(sv, max, count, [&](int k, const mlmq_server::Finished &f) {
+        tickets[k] = f.ticket;
+        statuses[k] = f.status;
+        if (solve_ns) solve_ns[k] = f.solve_ns;
+    });
+}
+
+extern "C" int mlmq_server_poll_results(mlmq_server *sv, mlmq_served_result *out, int max,
+                                        int *count) {
+    if (!sv || !count || (max > 0 && !out)) return MLMQ_ERR_ARG;
+    return server_poll(sv, max, count, [&](int k, const mlmq_server::Finished &f) {
+        out[k].ticket = f.ticket;
+        out[k].status = f.status;
+        out[k].solve_ns = f.solve_ns;
+        out[k].digest = f.digest;
+    });
+}
+
+extern "C" uint64_t mlmq_dist_digest(const int *dist, int64_t n) {
+    if (!dist || n <= 0) return 0;
+    unsigned long long sum = 0;
+    for (int64_t v = 0; v < n; v++) sum += digest_term((unsigned long long)v, dist[v]);
+    return sum;
 }
 
 extern "C" int mlmq_server_busy_slots(mlmq_server *sv, int *busy) {

@@ -52,6 +52,7 @@ class Server:
         self._tk = (ctypes.c_uint64 * 256)()
         self._st = (ctypes.c_int * 256)()
         self._ns = (ctypes.c_uint64 * 256)()
+        self._res = (_lib.ServedResult * 256)()
 
     def submit(self, dgraph, src, out, knobs=None):
         """Returns a ticket, or None when every slot is busy.  `out` must be a
@@ -84,6 +85,15 @@ class Server:
         check(lib.mlmq_server_poll_timed(self._h, self._tk, self._st, self._ns, 256,
                                          ctypes.byref(n)), "mlmq_server_poll_timed")
         return [(self._tk[i], self._st[i], self._ns[i] / 1e6) for i in range(n.value)]
+
+    def poll_results(self):
+        """[(ticket, status, solve_ms, digest)]: as poll_timed, with the
+        device-computed digest of each result's distances
+        (mlmq_dist_digest's definition; 0 for a failed query)."""
+        n = ctypes.c_int()
+        check(lib.mlmq_server_poll_results(self._h, self._res, 256, ctypes.byref(n)),
+              "mlmq_server_poll_results")
+        return [(r.ticket, r.status, r.solve_ns / 1e6, r.digest) for r in self._res[:n.value]]
 
     def busy(self):
         b = ctypes.c_int()
@@ -127,8 +137,9 @@ HOST_TIMEOUT = "host_timeout"
 
 def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300.0, knobs=None):
     """Runs the schedule against the server.  Returns a list of dicts
-    (arrival, start, finish, latency_s, solve_ms, graph, src, status[, dist]) in
-    schedule order; `keep(i)` selects the queries whose distances are kept;
+    (arrival, start, finish, latency_s, solve_ms, graph, src, status, digest
+    [, dist]) in schedule order, digest being the device-computed result
+    digest (None from a server without it); `keep(i)` selects the queries whose distances are kept;
     `knobs[graph index]` (optional) is that graph's per-query Config.
 
     A run that has not finished after `timeout_s` (host clock) stops there:
@@ -147,7 +158,8 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
             for i, buf, start in list(inflight.values()) + [(i, None, None) for i in pending]:
                 arr, gi, src = schedule[i]
                 out[i] = {"arrival": arr, "start": start, "finish": None, "latency_s": None,
-                          "solve_ms": None, "graph": gi, "src": src, "status": HOST_TIMEOUT}
+                          "solve_ms": None, "graph": gi, "src": src, "status": HOST_TIMEOUT,
+                          "digest": None}
             break
         # Admit arrived queries in arrival order while slots and buffers are
         # free; a query whose slot size is all taken is passed over (it keeps
@@ -179,12 +191,15 @@ def serve_poisson(server, dgraphs, schedule, keep=None, pool=None, timeout_s=300
                 continue
             inflight[tk] = (i, buf, now)
         pending.extendleft(reversed(skipped))
-        for tk, status, solve_ms in server.poll_timed():
+        done = (server.poll_results() if hasattr(server, "poll_results")
+                else [(*x, None) for x in server.poll_timed()])
+        for tk, status, solve_ms, digest in done:
             i, buf, start = inflight.pop(tk)
             arr, gi, src = schedule[i]
             fin = time.perf_counter() - t0
             rec = {"arrival": arr, "start": start, "finish": fin, "latency_s": fin - arr,
-                   "solve_ms": solve_ms, "graph": gi, "src": src, "status": status}
+                   "solve_ms": solve_ms, "graph": gi, "src": src, "status": status,
+                   "digest": digest}
             if keep is not None and keep(i):
                 view = buf[:dgraphs[gi].n]  # a torch tensor or a numpy array
                 rec["dist"] = (view.numpy() if hasattr(view, "numpy") else view).copy()

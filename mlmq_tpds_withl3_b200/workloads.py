@@ -40,6 +40,15 @@ def seeded_sources(g, count, seed=SEED, pool=None):
     return [int(v) for v in rng.choice(pool, size=count, replace=False)]
 
 
+def probe_sources(g, timed, count=4, seed=SEED + 1000, pool=None):
+    """`count` seeded sources for tuning, disjoint from the `timed` ones (a
+    configuration is picked on sources the measurement does not use), drawn
+    like seeded_sources from `pool` (default: the largest component)."""
+    pool = largest_component_vertices(g) if pool is None else np.asarray(pool)
+    pool = np.setdiff1d(pool, np.asarray(timed, dtype=pool.dtype))
+    return seeded_sources(g, count, seed=seed, pool=pool)
+
+
 def c1():
     return HostGraph.grid(512, 512, drop_p=0.10, wmin=1000, wmax=100000, seed=SEED), [0]
 
@@ -54,8 +63,12 @@ def c3(scale=22, nsrc=5):
     out-degree > 0 (a directed R-MAT vertex without out-arcs reaches only
     itself)."""
     g = HostGraph.rmat(scale, 16, 0.57, 0.19, 0.19, wmin=1, wmax=1 << 20, seed=SEED)
+    return g, seeded_sources(g, nsrc, pool=c3_source_pool(g))
+
+
+def c3_source_pool(g):
     comp = largest_component_vertices(g)
-    return g, seeded_sources(g, nsrc, pool=comp[np.diff(g.row)[comp] > 0])
+    return comp[np.diff(g.row)[comp] > 0]
 
 
 def c4(side=4896, nsrc=64):

@@ -246,3 +246,90 @@ int oracle_sssp_many(int n, const int *row, const int *col, const int *w, int ns
     pthread_mutex_destroy(&j.mu);
     return j.rc;
 }
+
+/* Fingerprint of a distance array, for checking results that are not kept
+ * in full (served queries): the sum, modulo 2^64, of
+ * splitmix64_out((v << 32) | (uint32)dist[v]) over every vertex v, where
+ * splitmix64_out is the output function of SplitMix64 (Steele, Lea and
+ * Flood, 2014).  The library computes the same sum on the device
+ * (mlmq_dist_digest defines it for callers); two arrays with equal digests
+ * are equal except with probability about 2^-64 per comparison. */
+static uint64_t splitmix64_out(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+uint64_t oracle_digest(int n, const int *dist) {
+    uint64_t s = 0;
+    for (int v = 0; v < n; v++) s += splitmix64_out(((uint64_t)(uint32_t)v << 32) | (uint32_t)dist[v]);
+    return s;
+}
+
+/* Many sources, keeping only each result's digest, total_work and reached
+ * count (memory: one distance array per thread). */
+typedef struct {
+    int n;
+    const int *row, *col, *w;
+    int nsrc;
+    const int *srcs;
+    uint64_t *digest;
+    long long *work;
+    int *reached;
+    int next;
+    int rc;
+    pthread_mutex_t mu;
+} digest_job;
+
+static void *digest_worker(void *arg) {
+    digest_job *j = (digest_job *)arg;
+    int *d = (int *)malloc(sizeof(int) * (size_t)j->n);
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        int k = j->next++;
+        if (!d && !j->rc) j->rc = ORACLE_ERR_NOMEM;
+        pthread_mutex_unlock(&j->mu);
+        if (k >= j->nsrc || !d) break;
+        long long wk = 0;
+        int rc = oracle_sssp_i32(j->n, j->row, j->col, j->w, j->srcs[k], d, &wk);
+        j->digest[k] = oracle_digest(j->n, d);
+        if (j->work) j->work[k] = wk;
+        if (j->reached) {
+            int c = 0;
+            for (int v = 0; v < j->n; v++) c += d[v] != INT_MAX;
+            j->reached[k] = c;
+        }
+        if (rc) {
+            pthread_mutex_lock(&j->mu);
+            if (!j->rc) j->rc = rc;
+            pthread_mutex_unlock(&j->mu);
+        }
+    }
+    free(d);
+    return NULL;
+}
+
+int oracle_sssp_digest_many(int n, const int *row, const int *col, const int *w, int nsrc,
+                            const int *srcs, uint64_t *digest, long long *work, int *reached,
+                            int nthreads) {
+    if (nsrc < 0 || (nsrc && (!srcs || !digest))) return ORACLE_ERR_ARG;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > nsrc) nthreads = nsrc ? nsrc : 1;
+    digest_job j;
+    j.n = n; j.row = row; j.col = col; j.w = w;
+    j.nsrc = nsrc; j.srcs = srcs; j.digest = digest; j.work = work; j.reached = reached;
+    j.next = 0; j.rc = 0;
+    pthread_mutex_init(&j.mu, NULL);
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nthreads);
+    if (!th) return ORACLE_ERR_NOMEM;
+    int started = 0;
+    for (int t = 0; t < nthreads; t++)
+        if (pthread_create(&th[t], NULL, digest_worker, &j) == 0) started++;
+        else break;
+    if (!started) digest_worker(&j);
+    for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
+    free(th);
+    pthread_mutex_destroy(&j.mu);
+    return j.rc;
+}

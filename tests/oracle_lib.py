@@ -31,6 +31,10 @@ def oracle():
                                         ctypes.POINTER(ctypes.c_longlong)]
         lib.oracle_sssp_many.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
                                          _vp, ctypes.c_int]
+        lib.oracle_digest.argtypes = [ctypes.c_int, _vp]
+        lib.oracle_digest.restype = ctypes.c_uint64
+        lib.oracle_sssp_digest_many.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp,
+                                                _vp, _vp, _vp, ctypes.c_int]
         _oracle = lib
     return _oracle
 
@@ -91,6 +95,43 @@ def sssp_many(g, sources, threads=None):
     if rc:
         raise RuntimeError(f"oracle_sssp_many rc={rc}")
     return d, work
+
+
+def digest(dist):
+    """oracle_digest of an int32 distance array (the fingerprint the library's
+    server reports for every served result)."""
+    d = _arr(dist.numpy() if hasattr(dist, "numpy") else dist)
+    return int(oracle().oracle_digest(len(d), d.ctypes.data))
+
+
+def digest_numpy(dist):
+    """The same fingerprint in numpy (an independent statement of it)."""
+    d = np.ascontiguousarray(dist, dtype=np.int32)
+    x = (np.arange(len(d), dtype=np.uint64) << np.uint64(32)) | d.view(np.uint32).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+        return int(np.sum(x, dtype=np.uint64))
+
+
+def sssp_digest_many(g, sources, threads=None):
+    """Many sources on a thread pool, keeping only each result's digest ->
+    (digest[nsrc] uint64, work[nsrc], reached[nsrc])."""
+    row, col, w = _arr(g.row), _arr(g.col), _arr(g.w)
+    n = len(row) - 1
+    srcs = _arr(sources)
+    dg = np.empty(len(srcs), np.uint64)
+    work = np.empty(len(srcs), np.int64)
+    reached = np.empty(len(srcs), np.int32)
+    threads = threads or os.cpu_count() or 1
+    rc = oracle().oracle_sssp_digest_many(n, row.ctypes.data, col.ctypes.data, w.ctypes.data,
+                                          len(srcs), srcs.ctypes.data, dg.ctypes.data,
+                                          work.ctypes.data, reached.ctypes.data, int(threads))
+    if rc:
+        raise RuntimeError(f"oracle_sssp_digest_many rc={rc}")
+    return dg, work, reached
 
 
 def ref_sequential(g, src):

@@ -43,14 +43,14 @@ def test_tuned_configurations_are_exact(tmp_path, monkeypatch):
     dg = DeviceGraph.upload(g)
     srcs = [0, 1, 2]
     ref, _ = oracle_lib.sssp_many(g, srcs)
-    cfg, rep = autotune.tune(dg, g, srcs[:2], kind="test-rmat", use_cache=True)
-    # at least: one delta, two CTA shapes, five single settings, the claim size
-    assert len(rep["trials"]) >= 9
+    cfg, rep = autotune.tune(dg, g, [3, 4, 5], kind="test-rmat", use_cache=True)
+    # seeds, deltas, two warp counts, three CTA counts, six options, the split, claims
+    assert len(rep["trials"]) >= 15 and rep["probe"] == [3, 4, 5]
     s = Solver(dg, cfg)
     for k, src in enumerate(srcs):
         assert np.array_equal(s.solve(src).dist(), ref[k]), (rep["config"], src)
     # the second call is served from the class cache
-    cfg2, rep2 = autotune.tune(dg, g, srcs[:2], kind="test-rmat", use_cache=True)
+    cfg2, rep2 = autotune.tune(dg, g, [3, 4, 5], kind="test-rmat", use_cache=True)
     assert rep2.get("cached") and cfg2.delta == cfg.delta
     qs = [(dg, x) for x in srcs]
     cands = [{"delta": 25000, "relax_unroll": 2, "topup": 16},
@@ -79,7 +79,8 @@ class _FakeSolver:
 def _tune_with_cost(monkeypatch, tmp_path, cost):
     monkeypatch.setenv("MLMQ_TUNE_CACHE", str(tmp_path / "tune.json"))
     monkeypatch.setattr(autotune, "Solver", _FakeSolver)
-    monkeypatch.setattr(autotune, "_time_solve", lambda s, src, reps=2: cost(s.cfg))
+    monkeypatch.setattr(autotune, "_time_solve", lambda s, src, reps=3: cost(s.cfg))
+    monkeypatch.setattr(autotune, "_sm_count", lambda: 148)
     g = HostGraph.grid(32, 32, seed=9)
     return autotune.tune(None, g, [0, 1], kind="fake", use_cache=False)
 
@@ -111,3 +112,46 @@ def test_tuner_tries_the_split_on_the_default_shape(monkeypatch, tmp_path):
     assert cfg.light_heavy == 1 and cfg.bucket_sync == 1
     tried = [t["config"] for t in rep["trials"]]
     assert any(t.get("l2_batch") == 16 for t in tried)
+
+
+def test_adaptive_seed_restates_the_reference_rule():
+    """core/include/adaptive.h:64-115 on graph_info: power-law graphs get
+    L1V_L2DQ with 8 buckets and delta = avg_weight - dev_weight; denser
+    graphs the L1V + unordered L2 stand-in; sparse ones delta = 5 x mean."""
+    from mlmq_tpds_withl3_b200 import MLMQ_L1V_L2DQ
+    r = HostGraph.rmat(14, seed=5)
+    info = r.info()
+    assert info.dev_nnz > 10
+    s = autotune.adaptive_seed(r)
+    assert s["queue_type"] == MLMQ_L1V_L2DQ and s["bucket_num"] == 8 and s["bucket_max"] == 4
+    assert s["delta"] == int(info.avg_weight - info.dev_weight) and s["l2_batch"] == 8
+    grid = HostGraph.grid(64, 64, drop_p=0.0, seed=3)  # degree 4 inside: avg_nnz > 3
+    sg = autotune.adaptive_seed(grid)
+    assert sg["queue_type"] == MLMQ_L1V_L2DQ and sg["bucket_num"] == 1
+    sparse = HostGraph.grid(64, 64, drop_p=0.3, seed=3)  # avg_nnz < 3
+    ss = autotune.adaptive_seed(sparse)
+    assert ss == {"delta": int(5 * sparse.info().avg_weight)}
+
+
+def test_tuner_tries_cta_counts_and_the_vector_l1_and_keeps_a_margin(monkeypatch, tmp_path):
+    from mlmq_tpds_withl3_b200 import MLMQ_L1V_L2DQ
+
+    def cost(c):
+        t = 2.0 - 0.5 * (c.get("work_blocks") == 296)
+        t -= 0.01 * (c.get("queue_type") == MLMQ_L1V_L2DQ)  # within the margin: not taken
+        return t
+    cfg, rep = _tune_with_cost(monkeypatch, tmp_path, cost)
+    tried = [t["config"] for t in rep["trials"]]
+    assert {74, 296, 444} <= {t.get("work_blocks") for t in tried}
+    assert any(t.get("queue_type") == MLMQ_L1V_L2DQ for t in tried)
+    assert rep["config"]["work_blocks"] == 296 and "queue_type" not in rep["config"]
+    assert cfg.work_blocks == 296
+
+
+def test_tuner_is_deterministic_for_equal_costs(monkeypatch, tmp_path):
+    """Two runs with the same timings pick the same configuration, and
+    near-equal candidates do not displace the first one found."""
+    cost = lambda c: 1.0 + 0.001 * (hash(json.dumps(c, sort_keys=True)) % 10)
+    a = _tune_with_cost(monkeypatch, tmp_path, cost)[1]["config"]
+    b = _tune_with_cost(monkeypatch, tmp_path, cost)[1]["config"]
+    assert a == b == {"delta": 200000}

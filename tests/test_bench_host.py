@@ -46,5 +46,21 @@ def test_peak_and_traffic_lookups():
 def test_default_arguments(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse()
-    assert a.gpus == 1 and a.workload == "c2" and a.impl != "reference"
-    assert a.warmup >= 3 and a.steps >= 1
+    assert a.gpus == 1 and a.workload == "all" and a.impl != "reference"
+    assert a.warmup >= 3 and a.steps >= 1 and a.skip == ""
+
+
+def test_both_arms_print_the_same_workload_config():
+    """The headline config holds workload keys only (solver settings go to
+    "solver"), so the reference arm, which never tunes, prints the same dict."""
+    from mlmq_tpds_withl3_b200 import HostGraph
+    g = HostGraph.grid(16, 16, seed=2)
+    a = bench.workload_config("c2", g, [0, 5], False)
+    b = bench.workload_config("c2", g, [0, 5], False)
+    assert a == b and set(a) == {"workload", "n", "m", "sources", "graph_sha256_16"}
+    assert bench.workload_config("c2", g, [0, 5], True)["workload"].endswith("[scaled down: --small]")
+
+
+def test_host_cpu_is_reported():
+    h = bench.host_cpu()
+    assert h["nproc"] >= 1 and isinstance(h["model"], str)

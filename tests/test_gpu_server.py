@@ -38,6 +38,8 @@ def test_served_results_equal_oracle_and_alone():
         # checks every solve the same way)
         ref, _ = oracle_lib.sssp_i32(hgs[gi], src)
         assert np.array_equal(r["dist"], ref), (i, gi, src)
+        # the device-computed digest of the same result
+        assert r["digest"] == oracle_lib.digest(ref), (i, gi, src)
     s = summarize(recs)
     assert s["errors"] == 0 and s["queries"] == 80 and s["finished"] == 80
 

@@ -96,3 +96,28 @@ def test_oracle_rejects_overflow():
         oracle_lib.sssp_i32(g, 0)
     with pytest.raises(RuntimeError):
         oracle_lib.sssp_i64(g, 0)
+
+
+def test_digest_statements_agree_and_separate_results():
+    """The served-result fingerprint, stated three times (oracle C, numpy,
+    the library's host function), gives one value per distance array, and
+    differs when one distance differs."""
+    from mlmq_tpds_withl3_b200._lib import dist_digest
+    g, _ = golden_graphs()["supplement2052"]
+    d, _ = oracle_lib.sssp_i32(g, 0)
+    a = oracle_lib.digest(d)
+    assert a == oracle_lib.digest_numpy(d) == dist_digest(d)
+    e = d.copy()
+    e[1025] += 1
+    assert oracle_lib.digest(e) != a
+    f = d.copy()
+    f[[3, 4]] = f[[4, 3]]  # the same values at other vertices
+    if f[3] != f[4]:
+        assert oracle_lib.digest(f) != a
+    # the digest of many sources equals the digests of the full results
+    srcs = [0, 1030, 2050]
+    dg, work, reached = oracle_lib.sssp_digest_many(g, srcs, threads=2)
+    full, works = oracle_lib.sssp_many(g, srcs)
+    assert [int(x) for x in dg] == [oracle_lib.digest(r) for r in full]
+    assert list(work) == list(works)
+    assert list(reached) == [int((r != oracle_lib.INT_MAX).sum()) for r in full]

@@ -69,6 +69,35 @@ def test_transforms_match_reference_checkers_directly():
     assert np.array_equal(rr.w, r.w)
 
 
+@pytest.mark.parametrize("case", range(6))
+def test_chain_shortcuts_equal_reference_on_seeded_graphs(case):
+    """Seeded grids (many chains), kNN and R-MAT graphs with random sources
+    and partition cuts: the pointer-jumping builder gives the reference
+    builder's graph (oracle/_ref/libref_chain.so) byte for byte, statistics
+    included."""
+    rng = np.random.default_rng(100 + case)
+    kind = case % 3
+    if kind == 0:
+        g = HostGraph.grid(int(rng.integers(40, 200)), int(rng.integers(40, 200)),
+                           drop_p=float(rng.uniform(0.2, 0.6)), seed=int(rng.integers(1e6)))
+    elif kind == 1:
+        g = HostGraph.knn(int(rng.integers(2000, 20000)), k=int(rng.integers(1, 3)),
+                          seed=int(rng.integers(1e6)))
+    else:
+        g = HostGraph.rmat(int(rng.integers(8, 12)), edge_factor=int(rng.integers(1, 4)),
+                           seed=int(rng.integers(1e6)))
+    src = int(rng.integers(g.n))
+    cut = int(rng.integers(0, g.n + 1)) if case >= 3 else g.n
+    ref = oracle_lib.ref_chain_shortcuts(g, src, cut)
+    if ref is None:
+        pytest.skip("reference-built checker not present")
+    row, col, w, st = ref
+    gp, mine = g.chain_shortcuts(source=src, cut=cut)
+    assert np.array_equal(gp.row, row) and np.array_equal(gp.col, col)
+    assert np.array_equal(gp.w, w)
+    assert list(mine.values()) == [int(x) for x in st]
+
+
 @pytest.mark.parametrize("name", ["grid64", "supplement2052", "components", "rmat11"])
 def test_transforms_keep_distances(name):
     g, sources = GRAPHS[name]
