@@ -268,6 +268,44 @@ def headline_workload(args):
     return name, g, srcs
 
 
+def _largest_component(g):
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+    a = csr_matrix((np.ones(g.m, np.int8), g.col, g.row), shape=(g.n, g.n))
+    _, labels = connected_components(a, directed=True, connection="weak")
+    return np.flatnonzero(labels == np.bincount(labels).argmax())
+
+
+def _seeded(pool, count, seed=1):
+    rng = np.random.default_rng(seed)
+    if count >= len(pool):
+        return [int(v) for v in pool[:count]]
+    return [int(v) for v in rng.choice(pool, size=count, replace=False)]
+
+
+def reference_workload(args):
+    """The headline graph and sources for the reference arm, built by the
+    oracle's C restatement of the generators (oracle/workload.c) so that the
+    reference arm never loads the product library; the source rule is the
+    one mlmq_tpds_withl3_b200.workloads applies (tests/test_bench_host.py
+    checks that both arms get the same graph and sources)."""
+    ol = oracle_lib()
+    name = args.workload if args.workload in ("c1", "c2", "c3") else "c2"
+    if name == "c1":
+        g, srcs = ol.gen_grid(512, 512, 0.10, 1000, 100000, 1), [0]
+    elif name == "c2":
+        g = ol.gen_knn(SMALL["c2_points"] if args.small else 6_300_000, 3, 1e6, 1)
+        srcs = _seeded(_largest_component(g), 5)
+    else:
+        g = ol.gen_rmat(SMALL["c3_scale"] if args.small else 22, 16, 0.57, 0.19, 0.19, 1,
+                        1 << 20, 1)
+        comp = _largest_component(g)
+        srcs = _seeded(comp[np.diff(g.row)[comp] > 0], 5)
+    if args.sources:
+        srcs = srcs[:args.sources]
+    return name, g, srcs
+
+
 def workload_config(name, g, srcs, small):
     """The workload keys of `config`, identical in both arms."""
     text = WORKLOAD_TEXT[name] + (" [scaled down: --small]" if small else "")
@@ -711,7 +749,7 @@ def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    name, g, srcs = headline_workload(args)
+    name, g, srcs = reference_workload(args)
     threads = max(1, min(len(srcs), os.cpu_count() or 1))
     for _ in range(args.warmup):
         cpu_reference_gteps(g, srcs, threads)

@@ -31,6 +31,9 @@ def oracle():
                                         ctypes.POINTER(ctypes.c_longlong)]
         lib.oracle_sssp_many.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
                                          _vp, ctypes.c_int]
+        for name in ("oracle_gen_grid", "oracle_gen_knn", "oracle_gen_rmat"):
+            getattr(lib, name).restype = ctypes.c_int
+        lib.oracle_free.argtypes = [_vp]
         lib.oracle_digest.argtypes = [ctypes.c_int, _vp]
         lib.oracle_digest.restype = ctypes.c_uint64
         lib.oracle_sssp_digest_many.argtypes = [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp,
@@ -95,6 +98,60 @@ def sssp_many(g, sources, threads=None):
     if rc:
         raise RuntimeError(f"oracle_sssp_many rc={rc}")
     return d, work
+
+
+class CsrGraph:
+    """A CSR graph held in numpy arrays (row n+1, col m, w m; int32)."""
+
+    def __init__(self, row, col, w, name="graph"):
+        self.row, self.col, self.w, self.name = row, col, w, name
+        self.n = len(row) - 1
+        self.m = len(col)
+
+
+def _generated(fn, args, name):
+    lib = oracle()
+    n = ctypes.c_int()
+    m = ctypes.c_longlong()
+    row, col, w = _vp(), _vp(), _vp()
+    rc = fn(*args, ctypes.byref(n), ctypes.byref(m), ctypes.byref(row), ctypes.byref(col),
+            ctypes.byref(w))
+    if rc:
+        raise RuntimeError(f"{name} rc={rc}")
+    try:
+        take = lambda p, k: np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_int32)),
+                                                  shape=(k,)).copy() if k else np.zeros(0, np.int32)
+        return CsrGraph(take(row, n.value + 1), take(col, m.value), take(w, m.value), name)
+    finally:
+        for p in (row, col, w):
+            lib.oracle_free(p)
+
+
+def gen_grid(width, height, drop_p=0.10, wmin=1000, wmax=100000, seed=1):
+    """oracle/workload.c's restatement of the road-like grid generator."""
+    lib = oracle()
+    return _generated(lib.oracle_gen_grid, (ctypes.c_int(width), ctypes.c_int(height),
+                                            ctypes.c_double(drop_p), ctypes.c_int(wmin),
+                                            ctypes.c_int(wmax), ctypes.c_uint64(seed)),
+                      f"grid{width}x{height}")
+
+
+def gen_knn(npoints, k=3, scale=1e6, seed=1):
+    """oracle/workload.c's restatement of the planar kNN generator."""
+    lib = oracle()
+    return _generated(lib.oracle_gen_knn, (ctypes.c_int(npoints), ctypes.c_int(k),
+                                           ctypes.c_double(scale), ctypes.c_uint64(seed)),
+                      f"knn{npoints}k{k}")
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, wmin=1, wmax=1 << 20, seed=1):
+    """oracle/workload.c's restatement of the R-MAT generator."""
+    lib = oracle()
+    return _generated(lib.oracle_gen_rmat, (ctypes.c_int(scale), ctypes.c_int(edge_factor),
+                                            ctypes.c_double(a), ctypes.c_double(b),
+                                            ctypes.c_double(c), ctypes.c_int(wmin),
+                                            ctypes.c_int(wmax), ctypes.c_uint64(seed)),
+                      f"rmat{scale}e{edge_factor}")
 
 
 def digest(dist):

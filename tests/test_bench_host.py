@@ -64,3 +64,32 @@ def test_both_arms_print_the_same_workload_config():
 def test_host_cpu_is_reported():
     h = bench.host_cpu()
     assert h["nproc"] >= 1 and isinstance(h["model"], str)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2", "c3"])
+def test_reference_arm_builds_the_same_workload_without_the_product(name, monkeypatch):
+    """The reference arm's graph (oracle/workload.c) and sources equal the GPU
+    arm's (mlmq_tpds_withl3_b200.workloads), on the scaled-down workloads."""
+    from mlmq_tpds_withl3_b200 import workloads
+    args = bench.parse(["--workload", name, "--small"])
+    rname, rg, rsrcs = bench.reference_workload(args)
+    gname, gg, gsrcs = bench.headline_workload(args)
+    assert rname == gname == name
+    assert bench.workload_config(name, rg, rsrcs, True) == bench.workload_config(name, gg, gsrcs, True)
+
+
+def test_reference_arm_does_not_load_the_product_library():
+    """bench.py --impl reference in a fresh process maps oracle libraries
+    only (checked through /proc/self/maps at the end of a tiny run)."""
+    import subprocess
+    code = ("import sys, runpy; sys.argv=['bench.py','--impl','reference','--workload','c1',"
+            "'--steps','1','--warmup','0'];"
+            "import bench; bench.main();"
+            "maps=open('/proc/self/maps').read();"
+            "print('PRODUCT' if 'libmlmq_b200' in maps else 'CLEAN')")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip().splitlines()[-1] == "CLEAN"
+    line = __import__("json").loads(out.stdout.strip().splitlines()[0])
+    assert line["impl"] == "reference" and line["config"]["n"] == 512 * 512
