@@ -98,6 +98,8 @@ def parse(argv=None):
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
     ap.add_argument("--side", type=int, default=0,
                     help="c4: grid side instead of 4896 (small cases for profiler captures)")
+    ap.add_argument("--scale", type=int, default=0,
+                    help="c3: R-MAT scale instead of 22 (small cases for profiler captures)")
     ap.add_argument("--batch-steps", type=int, default=10, help="batched: timed launches")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -262,7 +264,8 @@ def headline_workload(args):
     elif name == "c2":
         g, srcs = workloads.c2(points=SMALL["c2_points"]) if args.small else workloads.c2()
     else:
-        g, srcs = workloads.c3(scale=SMALL["c3_scale"]) if args.small else workloads.c3()
+        scale = args.scale or (SMALL["c3_scale"] if args.small else 22)
+        g, srcs = workloads.c3(scale=scale)
     if args.sources:
         srcs = srcs[:args.sources]
     return name, g, srcs
@@ -297,8 +300,8 @@ def reference_workload(args):
         g = ol.gen_knn(SMALL["c2_points"] if args.small else 6_300_000, 3, 1e6, 1)
         srcs = _seeded(_largest_component(g), 5)
     else:
-        g = ol.gen_rmat(SMALL["c3_scale"] if args.small else 22, 16, 0.57, 0.19, 0.19, 1,
-                        1 << 20, 1)
+        g = ol.gen_rmat(args.scale or (SMALL["c3_scale"] if args.small else 22), 16, 0.57, 0.19,
+                        0.19, 1, 1 << 20, 1)
         comp = _largest_component(g)
         srcs = _seeded(comp[np.diff(g.row)[comp] > 0], 5)
     if args.sources:
@@ -309,6 +312,8 @@ def reference_workload(args):
 def workload_config(name, g, srcs, small):
     """The workload keys of `config`, identical in both arms."""
     text = WORKLOAD_TEXT[name] + (" [scaled down: --small]" if small else "")
+    if name == "c3" and g.n != 1 << 22 and not small:
+        text = text.replace("scale 22", f"scale {g.n.bit_length() - 1} [scaled down: --scale]")
     return {"workload": text, "n": g.n, "m": g.m, "sources": [int(s) for s in srcs],
             "graph_sha256_16": graph_digest(g)}
 
@@ -447,6 +452,8 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
         "e2e": e2e, "cpu_baseline": cpu, "clocks": sampler.summary(),
         "gpu_launches": len(events), "wall_s_timed_region": t_wall,
         "relax_per_arc": float(stats["relaxed"]) / max(1.0, float(works[-1])),
+        "last_solve_stats": {k: int(stats[k]) for k in ("relaxed", "improved", "pushed",
+                                                         "l3_pushed", "batches", "idle")},
     }
     if tune_report:
         out["autotune"] = {"config": tune_report.get("config"),

@@ -115,7 +115,9 @@ typedef struct mlmq_config {
                             n + pieces + n in batches and servers; default 0 */
     int vertex_tiles;    /* 1 (default): read each vertex's adjacency from its
                             32-byte tile (up to 4 arcs inline, else its CSR
-                            range); 0: row offsets, then arcs */
+                            range); 2: 64-byte tiles with up to 8 arcs
+                            inline (built on first use, kept with the graph);
+                            0: row offsets, then arcs */
 } mlmq_config;
 
 /* Fills *cfg with the reference's defaults (common.h:24-34, sssp.cuh:20,
@@ -186,9 +188,25 @@ int mlmq_hgraph_write_gr(const mlmq_host_graph *g, const char *path);
  * invperm[old] = new (n entries each, may be NULL). */
 int mlmq_hgraph_reorder_bfs(const mlmq_host_graph *g, int root, mlmq_host_graph **out,
                             int *perm, int *invperm);
+/* The same reordering as a device preprocessing step (level-synchronous
+ * search that reproduces the FIFO discovery order exactly): the CSR in
+ * d_row/d_col/d_w (device, current device) is written reordered to
+ * d_row_out[n+1], d_col_out[m], d_w_out[m], with d_perm[new] = old and
+ * d_invperm[old] = new (n each), on `stream` (a cudaStream_t; NULL = legacy
+ * default stream).  Temporary device memory comes from the library's pool.
+ * Returns when the result is complete.  Output equals
+ * mlmq_hgraph_reorder_bfs byte for byte. */
+int mlmq_reorder_bfs_device(int n, int64_t m, const int *d_row, const int *d_col, const int *d_w,
+                            int root, int *d_row_out, int *d_col_out, int *d_w_out, int *d_perm,
+                            int *d_invperm, void *stream);
+/* mlmq_hgraph_reorder_bfs computed on the current device: the host graph is
+ * copied over, reordered by mlmq_reorder_bfs_device and copied back. */
+int mlmq_hgraph_reorder_bfs_gpu(const mlmq_host_graph *g, int root, mlmq_host_graph **out,
+                                int *perm, int *invperm);
 /* Chain-shortcut augmentation G+ (SSSP/l3/l3_chain_shortcuts.h:23-109):
  * adds one arc per maximal walk through degree-2 chain vertices, keeps every
- * original arc, so distances are unchanged.  cut = n places no partition
+ * original arc, so distances are unchanged.  The output equals the reference
+ * builder's byte for byte; the walks are resolved by pointer jumping.  cut = n places no partition
  * restriction; stats (may be NULL): chain vertices, shortcuts, longest walk,
  * walks dropped for INT_MAX overflow, arcs represented. */
 int mlmq_hgraph_chain_shortcuts(const mlmq_host_graph *g, int cut, int source,
@@ -231,6 +249,11 @@ int mlmq_graph_pieces(const mlmq_graph *g, int *pieces);
  * the server (mlmq_server_submit_cfg returns MLMQ_ERR_STATE otherwise).
  * Likewise bind graphs before a server starts on the same device. */
 int mlmq_graph_prepare_light(const mlmq_graph *g, int delta);
+/* Builds (once, kept with the graph) the tile array of a vertex_tiles
+ * setting: only 2 (wide tiles) needs building; solvers and batches do it on
+ * first use, a server cannot (as for mlmq_graph_prepare_light): prepare
+ * before the server starts. */
+int mlmq_graph_prepare_tiles(const mlmq_graph *g, int vertex_tiles);
 void mlmq_graph_free(mlmq_graph *g);
 
 /* A solver owns one distance array and one queue workspace on the device

@@ -107,12 +107,16 @@ _sig("mlmq_hgraph_view", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_i6
 _sig("mlmq_hgraph_free", None, c_vp)
 _sig("mlmq_hgraph_reorder_bfs", c_int, c_vp, c_int, ctypes.POINTER(c_vp), c_vp, c_vp)
 _sig("mlmq_hgraph_chain_shortcuts", c_int, c_vp, c_int, c_int, ctypes.POINTER(c_vp), c_vp)
+_sig("mlmq_hgraph_reorder_bfs_gpu", c_int, c_vp, c_int, ctypes.POINTER(c_vp), c_vp, c_vp)
+_sig("mlmq_reorder_bfs_device", c_int, c_int, c_i64, c_vp, c_vp, c_vp, c_int, c_vp, c_vp, c_vp,
+     c_vp, c_vp, c_vp)
 # device graphs / solver
 _sig("mlmq_graph_upload", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp))
 _sig("mlmq_graph_wrap_device", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp))
 _sig("mlmq_graph_size", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_i64))
 _sig("mlmq_graph_pieces", c_int, c_vp, ctypes.POINTER(c_int))
 _sig("mlmq_graph_prepare_light", c_int, c_vp, c_int)
+_sig("mlmq_graph_prepare_tiles", c_int, c_vp, c_int)
 _sig("mlmq_graph_free", None, c_vp)
 _sig("mlmq_release_cached", c_int)
 _sig("mlmq_solver_create", c_int, c_vp, ctypes.POINTER(Config), ctypes.POINTER(c_vp))

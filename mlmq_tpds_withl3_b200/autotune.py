@@ -134,8 +134,11 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
       shape     8 or 24 worker warps per CTA, then the CTA count (the
                 reference's MLMQ_WORK_BLOCKS): half the SMs, one per SM, or
                 two and three per SM where they fit;
-      options   1 or 2 relaxation rounds in flight, vertex tiles off, the L1
-                run-ahead bound off or 16, the vector L1 (L1V_L2DQ);
+      options   1 or 2 relaxation rounds in flight, vertex tiles off or
+                64-byte (8 inline arcs), warp-cooperative relaxation from
+                degree 64 or never (the reference's LARGEV is 16; above it a
+                warp relaxes one vertex at a time), the L1 run-ahead bound off
+                or 16, the vector L1 (L1V_L2DQ);
       split     the light/heavy split with bulk-synchronous buckets at the
                 best delta and a quarter of it, on the shape found so far
                 and on the default one (greedy stages can pick a shape that
@@ -183,6 +186,7 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         consider({**best, "work_blocks": wb})
     from ._lib import MLMQ_L1V_L2DQ
     for opt in ({"relax_unroll": 1}, {"relax_unroll": 2}, {"vertex_tiles": 0},
+                {"vertex_tiles": 2}, {"large_degree": 64}, {"large_degree": 4096},
                 {"l1_ahead": 0}, {"l1_ahead": 16}, {"queue_type": MLMQ_L1V_L2DQ}):
         consider({**best, **opt})
     if best.get("vertex_tiles", 1):

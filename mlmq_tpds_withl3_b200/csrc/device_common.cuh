@@ -13,8 +13,10 @@ constexpr int NB_MAX = 32;      // L2 buckets; lane b of a warp owns bucket b's 
 constexpr int L1_CAP = 64;      // SLF ring slots per warp (reference MAX_L1SLF_BATCH_SIZE)
 constexpr unsigned long long SENT = ~0ull;  // empty ring slot
 // Vertex tiles: 32 bytes per vertex, {dst, weight} x TILE_ARCS inline (unused
-// slots dst = -1), or {TILE_CSR, first arc, degree, ...} for higher degree.
+// slots dst = -1), or {TILE_CSR, first arc, degree, ...} for higher degree;
+// wide tiles are 64 bytes with up to TILE_ARCS_WIDE arcs inline.
 constexpr int TILE_ARCS = 4;
+constexpr int TILE_ARCS_WIDE = 8;
 constexpr int TILE_CSR = -2;
 // A vertex of more than SPLIT_MIN arcs is relaxed as pieces of at most
 // PIECE_ARCS arcs.  Piece k of the graph is a virtual vertex id n + k with
@@ -27,7 +29,7 @@ constexpr int PIECE_ARCS = 512;
 // staged tile arcs, outbox of records bound for L2/L3, winners of the
 // relaxation rounds in flight (at most 4 rounds of 32).
 constexpr int OUTBOX_CAP = 64;
-constexpr int OUTBOX_OFF = L1_CAP + 32 + 32 * TILE_ARCS;
+constexpr int OUTBOX_OFF = L1_CAP + 32 + 32 * TILE_ARCS_WIDE;
 constexpr int WINBUF_CAP = 128;
 constexpr int WINBUF_OFF = OUTBOX_OFF + OUTBOX_CAP;
 constexpr int WARP_SMEM_SLOTS = WINBUF_OFF + WINBUF_CAP;

@@ -28,11 +28,7 @@
 #include <thread>
 #include <vector>
 
-struct mlmq_host_graph {
-    int n = 0;
-    int64_t m = 0;
-    std::vector<int> row, col, w, perm;
-};
+#include "host_graph.h"
 
 namespace {
 

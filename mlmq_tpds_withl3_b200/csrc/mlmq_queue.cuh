@@ -59,7 +59,8 @@ struct PlainParams {
     int nids;    // nslots, + n with the light/heavy split (ids nslots + v: v's heavy record)
     const int *__restrict__ row;
     const int2 *__restrict__ arcs;  // interleaved {dst, weight} (ArcsInterleaved)
-    const int4 *__restrict__ tiles; // 2 per vertex, or null: read row offsets instead
+    const int4 *__restrict__ tiles; // tile_stride per vertex, or null: read row offsets instead
+    int tile_stride;                // int4 per tile: 2 (4 inline arcs) or 4 (8 inline arcs)
     const int *__restrict__ col;    // caller's CSR arrays, read in place (ArcsSplit)
     const int *__restrict__ w;
     int *dist;
@@ -454,7 +455,7 @@ __device__ __forceinline__ int l3_rebucket(const PlainParams &p, WarpQ &q, volat
             dv = v - (unsigned)p.nslots;
             add = p.delta;
         } else if (v >= (unsigned)p.n) {
-            dv = (unsigned)__ldg(p.tiles + 2 * (size_t)v).w;
+            dv = (unsigned)__ldg(p.tiles + (size_t)p.tile_stride * v).w;
         }
         const unsigned long long now = (unsigned long long)(unsigned)__ldcg(p.dist + dv) + add;
         cur = (unsigned)min(now, (unsigned long long)rec_d(r));
@@ -594,7 +595,7 @@ __device__ __forceinline__ void push_pieces(const PlainParams &p, WarpQ &q, int 
 }
 
 // Relaxes up to 32 records (one per lane) and feeds the winners to L1.
-// `stage` is this warp's TILE_ARCS * 32 arcs of shared memory.
+// `stage` is this warp's TILE_ARCS_WIDE * 32 arcs of shared memory.
 template <class Arcs, int K>
 __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint2 *ring,
                                             int2 *stage, bool valid, unsigned v, unsigned d) {
@@ -625,12 +626,18 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
         // INT_MIN + its stage offset, so the arc distribution below handles
         // staged and CSR arcs alike and keeps the CSR path's arc order.
         int cur = INT_MAX, light = 0;
-        int4 ta = make_int4(-1, 0, -1, 0), tb = ta;
+        int4 ta = make_int4(-1, 0, -1, 0), tb = ta, tc = ta, td = ta;
         const bool piece = valid && v >= (unsigned)p.n;
+        const bool wide = p.tile_stride == 4;
         if (valid) {
             if (!piece) cur = __ldcg(p.dist + v);
-            ta = __ldg(p.tiles + 2 * (size_t)v);
-            tb = __ldg(p.tiles + 2 * (size_t)v + 1);
+            const int4 *t = p.tiles + (size_t)p.tile_stride * v;
+            ta = __ldg(t);
+            tb = __ldg(t + 1);
+            if (wide) {
+                tc = __ldg(t + 2);
+                td = __ldg(t + 3);
+            }
             if (p.split && !piece) light = __ldg(p.split + v);
         }
         if (piece) cur = __ldcg(p.dist + ta.w);  // a piece is as fresh as its owner
@@ -667,19 +674,29 @@ __device__ __forceinline__ void relax_batch(const PlainParams &p, WarpQ &q, uint
                     }
                 }
             } else {
-                int2 *st = stage + TILE_ARCS * lane;
+                int2 *st = stage + TILE_ARCS_WIDE * lane;
                 st[0] = make_int2(ta.x, ta.y);
                 st[1] = make_int2(ta.z, ta.w);
                 st[2] = make_int2(tb.x, tb.y);
                 st[3] = make_int2(tb.z, tb.w);
-                const int cnt = (ta.x >= 0) + (ta.z >= 0) + (tb.x >= 0) + (tb.z >= 0);
-                beg = INT_MIN + TILE_ARCS * lane;
+                int cnt = (ta.x >= 0) + (ta.z >= 0) + (tb.x >= 0) + (tb.z >= 0);
+                if (wide) {
+                    st[4] = make_int2(tc.x, tc.y);
+                    st[5] = make_int2(tc.z, tc.w);
+                    st[6] = make_int2(td.x, td.y);
+                    st[7] = make_int2(td.z, td.w);
+                    cnt += (tc.x >= 0) + (tc.z >= 0) + (td.x >= 0) + (td.z >= 0);
+                }
+                beg = INT_MIN + TILE_ARCS_WIDE * lane;
                 deg = cnt;
                 if (lh) {
                     // inline arcs are sorted by weight too
                     const unsigned dl = p.delta;
-                    const int nl = (cnt > 0 && (unsigned)ta.y < dl) + (cnt > 1 && (unsigned)ta.w < dl) +
-                                   (cnt > 2 && (unsigned)tb.y < dl) + (cnt > 3 && (unsigned)tb.w < dl);
+                    int nl = (cnt > 0 && (unsigned)ta.y < dl) + (cnt > 1 && (unsigned)ta.w < dl) +
+                             (cnt > 2 && (unsigned)tb.y < dl) + (cnt > 3 && (unsigned)tb.w < dl);
+                    if (wide)
+                        nl += (cnt > 4 && (unsigned)tc.y < dl) + (cnt > 5 && (unsigned)tc.w < dl) +
+                              (cnt > 6 && (unsigned)td.y < dl) + (cnt > 7 && (unsigned)td.w < dl);
                     if (heavyrec) {
                         beg += nl;
                         deg = cnt - nl;

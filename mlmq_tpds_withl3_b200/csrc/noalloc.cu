@@ -181,6 +181,7 @@ extern "C" int mlmq_sssp_solve_noalloc(int n, int m, const int *d_row, const int
     p.row = d_row;
     p.arcs = nullptr;
     p.tiles = nullptr;  // the caller's CSR is read in place
+    p.tile_stride = 2;
     p.col = d_col;
     p.w = d_w;
     p.dist = d_dist;

@@ -181,6 +181,36 @@ __global__ void tile_kernel(const int *__restrict__ row, const int2 *__restrict_
     }
 }
 
+// Wide tiles from the 32-byte ones: a vertex of at most TILE_ARCS_WIDE arcs
+// gets them inline (its arcs in the same weight order), every other tile
+// (CSR range, split vertex, piece) is copied with the extra slots empty.
+__global__ void widen_tiles_kernel(const int4 *__restrict__ tiles, const int2 *__restrict__ arcs,
+                                   int n, int slots, int4 *wide) {
+    const int4 none = make_int4(-1, 0, -1, 0);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < slots; v += gridDim.x * blockDim.x) {
+        const int4 t0 = tiles[2 * (size_t)v], t1 = tiles[2 * (size_t)v + 1];
+        int4 *o = wide + 4 * (size_t)v;
+        if (v < n && t0.x == TILE_CSR && t0.z <= TILE_ARCS_WIDE) {
+            int t[16];
+            for (int i = 0; i < 16; i += 2) {
+                t[i] = -1;
+                t[i + 1] = 0;
+            }
+            for (int i = 0; i < t0.z; i++) {
+                const int2 a = arcs[t0.y + i];
+                t[2 * i] = a.x;
+                t[2 * i + 1] = a.y;
+            }
+            for (int q = 0; q < 4; q++) o[q] = make_int4(t[4 * q], t[4 * q + 1], t[4 * q + 2], t[4 * q + 3]);
+        } else {
+            o[0] = t0;
+            o[1] = (v < n && t0.x >= -1) ? t1 : none;  // inline arcs keep their second half
+            o[2] = none;
+            o[3] = none;
+        }
+    }
+}
+
 // Light arcs (weight < delta) of each vertex: a lower bound search in its
 // weight-sorted arcs.
 // Vertices of more than SPLIT_MIN arcs as {vertex, first arc, degree, 0}, in
@@ -288,6 +318,46 @@ int graph_light_split(const mlmq_graph *gc, int delta, const int **out) {
     return MLMQ_OK;
 }
 
+int graph_tiles_cached(const mlmq_graph *gc, int vertex_tiles, const int4 **out, int *stride) {
+    *out = nullptr;
+    *stride = 2;
+    if (vertex_tiles == 0) return MLMQ_OK;
+    if (vertex_tiles == 1) {
+        *out = gc->d_tiles;
+        return MLMQ_OK;
+    }
+    auto *g = const_cast<mlmq_graph *>(gc);
+    std::lock_guard<std::mutex> lk(g->split_mu);
+    if (!g->d_tiles_wide) return MLMQ_ERR_STATE;
+    *out = g->d_tiles_wide;
+    *stride = 4;
+    return MLMQ_OK;
+}
+
+int graph_tiles(const mlmq_graph *gc, int vertex_tiles, const int4 **out, int *stride) {
+    if (vertex_tiles != 2) return graph_tiles_cached(gc, vertex_tiles, out, stride);
+    auto *g = const_cast<mlmq_graph *>(gc);
+    std::lock_guard<std::mutex> lk(g->split_mu);
+    if (!g->d_tiles_wide) {
+        int4 *d = nullptr;
+        int rc = dev_alloc(&d, 4 * sizeof(int4) * (size_t)g->slots(), 0, "alloc(wide tiles)");
+        if (!rc) {
+            const int blocks = (int)std::min<int64_t>(((int64_t)g->slots() + 255) / 256, 148 * 16);
+            widen_tiles_kernel<<<blocks, 256>>>(g->d_tiles, g->d_arcs, g->n, g->slots(), d);
+            rc = cuda_fail(cudaGetLastError(), "wide tiles launch");
+            if (!rc) rc = cuda_fail(cudaStreamSynchronize(0), "wide tiles");
+        }
+        if (rc) {
+            dev_free(d, 0);
+            return rc;
+        }
+        g->d_tiles_wide = d;
+    }
+    *out = g->d_tiles_wide;
+    *stride = 4;
+    return MLMQ_OK;
+}
+
 int fill_device(int *p, int64_t n, int v, cudaStream_t s) {
     if (n <= 0) return MLMQ_OK;
     int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
@@ -316,7 +386,7 @@ int validate_config(const mlmq_config &c) {
     if (c.relax_precheck != 0 && c.relax_precheck != 1) return MLMQ_ERR_ARG;
     if (c.relax_unroll != 1 && c.relax_unroll != 2 && c.relax_unroll != 4) return MLMQ_ERR_ARG;
     if (c.relax_unroll > 1 && c.warps_per_block > MLMQ_MAX_UNROLLED_WARPS) return MLMQ_ERR_ARG;
-    if (c.vertex_tiles != 0 && c.vertex_tiles != 1) return MLMQ_ERR_ARG;
+    if (c.vertex_tiles < 0 || c.vertex_tiles > 2) return MLMQ_ERR_ARG;
     if (c.l1_ahead < 0) return MLMQ_ERR_ARG;
     if (c.topup < 0 || c.topup > 32) return MLMQ_ERR_ARG;
     if (c.bucket_sync != 0 && c.bucket_sync != 1) return MLMQ_ERR_ARG;
@@ -595,6 +665,13 @@ extern "C" int mlmq_graph_prepare_light(const mlmq_graph *g, int delta) {
     return graph_light_split(g, delta, &d);
 }
 
+extern "C" int mlmq_graph_prepare_tiles(const mlmq_graph *g, int vertex_tiles) {
+    if (!g || vertex_tiles < 0 || vertex_tiles > 2) return MLMQ_ERR_ARG;
+    const int4 *t = nullptr;
+    int stride = 0;
+    return graph_tiles(g, vertex_tiles, &t, &stride);
+}
+
 extern "C" int mlmq_graph_pieces(const mlmq_graph *g, int *pieces) {
     if (!g || !pieces) return MLMQ_ERR_ARG;
     *pieces = g->pieces;
@@ -624,6 +701,7 @@ void graph_release(const mlmq_graph *gc) {
     // waiting for unrelated work on the device.
     dev_free(g->d_arcs, 0);
     dev_free(g->d_tiles, 0);
+    dev_free(g->d_tiles_wide, 0);
     for (auto &e : g->split_cache) dev_free(e.second, 0);
     if (g->own_row) dev_free(g->d_row, 0);
     delete g;
@@ -657,6 +735,10 @@ extern "C" int mlmq_solver_create(const mlmq_graph *g, const mlmq_config *cfg_in
                                 : std::min(24, std::max(MLMQ_MIN_RING_LOG2, ceil_log2(m / 2 + 1)));
     s->nids = g->slots() + (cfg.light_heavy ? g->n : 0);
     if (cfg.light_heavy && (rc = graph_light_split(g, cfg.delta, &s->split))) {
+        mlmq_solver_destroy(s);
+        return rc;
+    }
+    if ((rc = graph_tiles(g, cfg.vertex_tiles, &s->tiles, &s->tile_stride))) {
         mlmq_solver_destroy(s);
         return rc;
     }
@@ -728,7 +810,8 @@ extern "C" int mlmq_solver_launch(mlmq_solver *s, int src, void *stream) {
     p.nids = s->nids;
     p.row = s->g->d_row;
     p.arcs = s->g->d_arcs;
-    p.tiles = s->cfg.vertex_tiles ? s->g->d_tiles : nullptr;
+    p.tiles = s->tiles;
+    p.tile_stride = s->tile_stride;
     p.col = nullptr;
     p.w = nullptr;
     p.dist = s->d_dist;

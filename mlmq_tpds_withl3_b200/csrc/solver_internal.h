@@ -30,6 +30,9 @@ struct mlmq_graph {
     // Per delta: light arcs (weight < delta) of each vertex, n ints.
     std::mutex split_mu;
     std::vector<std::pair<int, int *>> split_cache;
+    // Wide tiles (4 per vertex and per piece, up to 8 arcs inline), built on
+    // first use from d_tiles (guarded by split_mu).
+    int4 *d_tiles_wide = nullptr;
 };
 
 struct mlmq_solver {
@@ -40,6 +43,8 @@ struct mlmq_solver {
     int l2_log = 0, l3_log = 0;
     int nids = 0;               // queue ids: vertex slots, + n with the light/heavy split
     const int *split = nullptr; // light arcs per vertex for cfg.delta (owned by the graph)
+    const int4 *tiles = nullptr; // tile array for cfg.vertex_tiles (owned by the graph)
+    int tile_stride = 2;
     int *d_dist = nullptr;
     unsigned long long *d_l2 = nullptr;
     unsigned long long *d_l3 = nullptr;
@@ -92,6 +97,11 @@ int fill_device(int *p, int64_t n, int v, cudaStream_t s);
 int graph_light_split(const mlmq_graph *g, int delta, const int **out);
 // The same when already computed, else MLMQ_ERR_STATE (launches nothing).
 int graph_light_split_cached(const mlmq_graph *g, int delta, const int **out);
+// The tile array a configuration reads (vertex_tiles 1: d_tiles; 2: the
+// wide tiles, built on first use; 0: none) and its int4 per tile.
+int graph_tiles(const mlmq_graph *g, int vertex_tiles, const int4 **out, int *stride);
+// The same without building anything (MLMQ_ERR_STATE if not built yet).
+int graph_tiles_cached(const mlmq_graph *g, int vertex_tiles, const int4 **out, int *stride);
 int validate_config(const mlmq_config &c);
 int status_to_error(unsigned st);
 int device_sm_count(int *sms);

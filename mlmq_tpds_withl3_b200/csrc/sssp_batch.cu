@@ -165,6 +165,7 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     p.l1_ahead = b->cfg.l1_ahead;
     p.topup = b->cfg.topup;
     p.bucket_sync = b->cfg.bucket_sync;
+    p.tile_stride = b->cfg.vertex_tiles == 2 ? 4 : 2;
     p.split = nullptr;  // per query
     p.precheck = b->cfg.relax_precheck;
     p.delta = (unsigned)b->cfg.delta;
@@ -300,7 +301,8 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
         BatchQuery &qy = b->h_queries[q];
         qy.row = g->d_row;
         qy.arcs = g->d_arcs;
-        qy.tiles = b->cfg.vertex_tiles ? g->d_tiles : nullptr;
+        int stride = 2;
+        if ((rc = graph_tiles(g, b->cfg.vertex_tiles, &qy.tiles, &stride))) return rc;
         qy.n = g->n;
         qy.nslots = g->slots();
         qy.nids = g->slots() + (b->cfg.light_heavy ? g->n : 0);

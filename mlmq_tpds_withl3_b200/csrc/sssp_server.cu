@@ -519,6 +519,7 @@ int server_create(int slots, const int *layout, int max_vertices, const mlmq_con
         b.l1_ahead = cfg.l1_ahead;
         b.topup = cfg.topup;
         b.bucket_sync = cfg.bucket_sync;
+        b.tile_stride = cfg.vertex_tiles == 2 ? 4 : 2;
         b.split = nullptr;  // per query
         b.precheck = cfg.relax_precheck;
         b.delta = (unsigned)cfg.delta;
@@ -622,6 +623,10 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
         const int rc = graph_light_split_cached(g, k.delta, &split);
         if (rc) return rc;
     }
+    // Likewise the wide tiles (mlmq_graph_prepare_tiles).
+    const int4 *tiles = nullptr;
+    int stride = 2;
+    if (int rc = graph_tiles_cached(g, sv->cfg.vertex_tiles, &tiles, &stride)) return rc;
     // The smallest free slot with at least the CTAs the query asks for
     // (knobs->work_blocks; 0 or no knobs: any).
     const int want = knobs ? knobs->work_blocks : 0;
@@ -640,7 +645,7 @@ extern "C" int mlmq_server_submit_cfg(mlmq_server *sv, const mlmq_graph *g, int 
     SlotCommand &cmd = sv->h_cmd[free_slot];
     cmd.row = g->d_row;
     cmd.arcs = g->d_arcs;
-    cmd.tiles = sv->cfg.vertex_tiles ? g->d_tiles : nullptr;
+    cmd.tiles = tiles;
     cmd.n = g->n;
     cmd.nslots = g->slots();
     cmd.src = src;

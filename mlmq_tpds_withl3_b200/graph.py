@@ -116,6 +116,17 @@ class HostGraph:
                                           inv.ctypes.data), "mlmq_hgraph_reorder_bfs")
         return HostGraph(h.value, f"{self.name}.bfs{root}"), perm, inv
 
+    def reorder_bfs_gpu(self, root=0):
+        """reorder_bfs computed on the current CUDA device
+        (mlmq_hgraph_reorder_bfs_gpu); the same output."""
+        h = ctypes.c_void_p()
+        perm = np.empty(self.n, dtype=np.int32)
+        inv = np.empty(self.n, dtype=np.int32)
+        check(lib.mlmq_hgraph_reorder_bfs_gpu(self._h, int(root), ctypes.byref(h),
+                                              perm.ctypes.data, inv.ctypes.data),
+              "mlmq_hgraph_reorder_bfs_gpu")
+        return HostGraph(h.value, f"{self.name}.bfs{root}"), perm, inv
+
     def chain_shortcuts(self, source=0, cut=None):
         """Chain-shortcut augmentation G+ (reference
         SSSP/l3/l3_chain_shortcuts.h:23-109): one extra arc per maximal walk

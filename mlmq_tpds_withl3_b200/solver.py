@@ -56,6 +56,11 @@ class DeviceGraph:
         before a server that runs light_heavy queries on this graph starts)."""
         check(lib.mlmq_graph_prepare_light(self._h, int(delta)), "mlmq_graph_prepare_light")
 
+    def prepare_tiles(self, vertex_tiles):
+        """The tile array of a vertex_tiles setting (2: 64-byte tiles with up
+        to 8 inline arcs), needed before a server with that setting starts."""
+        check(lib.mlmq_graph_prepare_tiles(self._h, int(vertex_tiles)), "mlmq_graph_prepare_tiles")
+
     def close(self):
         if self._h is not None and self._h.value:
             lib.mlmq_graph_free(self._h)

@@ -44,8 +44,8 @@ def test_tuned_configurations_are_exact(tmp_path, monkeypatch):
     srcs = [0, 1, 2]
     ref, _ = oracle_lib.sssp_many(g, srcs)
     cfg, rep = autotune.tune(dg, g, [3, 4, 5], kind="test-rmat", use_cache=True)
-    # seeds, deltas, two warp counts, three CTA counts, six options, the split, claims
-    assert len(rep["trials"]) >= 15 and rep["probe"] == [3, 4, 5]
+    # seeds, deltas, two warp counts, three CTA counts, nine options, the split, claims
+    assert len(rep["trials"]) >= 18 and rep["probe"] == [3, 4, 5]
     s = Solver(dg, cfg)
     for k, src in enumerate(srcs):
         assert np.array_equal(s.solve(src).dist(), ref[k]), (rep["config"], src)
@@ -144,6 +144,8 @@ def test_tuner_tries_cta_counts_and_the_vector_l1_and_keeps_a_margin(monkeypatch
     tried = [t["config"] for t in rep["trials"]]
     assert {74, 296, 444} <= {t.get("work_blocks") for t in tried}
     assert any(t.get("queue_type") == MLMQ_L1V_L2DQ for t in tried)
+    assert {0, 2} <= {t.get("vertex_tiles") for t in tried}
+    assert {64, 4096} <= {t.get("large_degree") for t in tried}
     assert rep["config"]["work_blocks"] == 296 and "queue_type" not in rep["config"]
     assert cfg.work_blocks == 296
 

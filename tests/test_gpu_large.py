@@ -1,0 +1,76 @@
+"""Parity at the largest sizes one test process checks in seconds: every
+result of an R-MAT scale-20 plain solve (5 sources), of a 64-query batched
+launch on a 2048 x 2048 road-like grid, and of a served mix of graphs up to
+2^20 vertices is compared with the CPU oracle (exact int32 equality; the
+reference checks every solve the same way, SS/SSSP/sssp_run.cu:849-859 and
+SS/SSSP/main.cu:131-144)."""
+import time
+
+import numpy as np
+import pytest
+
+import oracle_lib
+from mlmq_tpds_withl3_b200 import BatchSolver, DeviceGraph, HostGraph, Solver, default_config
+from mlmq_tpds_withl3_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def test_rmat20_five_sources_every_result_exact():
+    g = HostGraph.rmat(20, 16, 0.57, 0.19, 0.19, wmin=1, wmax=1 << 20, seed=1)
+    srcs = workloads.seeded_sources(g, 5, pool=workloads.c3_source_pool(g))
+    ref, _ = oracle_lib.sssp_many(g, srcs)
+    dg = DeviceGraph.upload(g)
+    for cfg in ({}, {"delta": 200000, "warps_per_block": 24, "relax_unroll": 2, "l1_ahead": 0},
+                {"delta": 50000, "light_heavy": 1, "bucket_sync": 1, "l2_batch": 16},
+                {"large_degree": 4096, "work_blocks": 296, "warps_per_block": 8}):
+        s = Solver(dg, cfg)
+        for k, src in enumerate(srcs):
+            assert np.array_equal(s.solve(src).dist(), ref[k]), (cfg, src)
+        s.close()
+    dg.close()
+
+
+def test_batched_2048_grid_64_queries_every_result_exact():
+    g, srcs = workloads.c4(side=2048, nsrc=64)
+    ref, _ = oracle_lib.sssp_many(g, srcs)
+    dg = DeviceGraph.upload(g)
+    cfg = default_config(delta=25000, warps_per_block=8, relax_unroll=2, topup=16,
+                         l2_cap_log2=20, l2_batch=16, bucket_max=2)
+    b = BatchSolver(len(srcs), dg.slots, cfg)
+    queries = [(dg, s) for s in srcs]
+    for replay in range(2):  # captured launch, then its replay
+        b.run(queries, use_graph=True)
+        for q in range(len(srcs)):
+            assert np.array_equal(b.dist(q), ref[q]), (replay, q)
+    b.close()
+    dg.close()
+
+
+def test_served_mix_up_to_2pow20_every_result_exact():
+    """Graphs of 2^16..2^20 vertices (grids and R-MAT) resident, 300 Poisson
+    arrivals: every served result equals the oracle, element by element and
+    by the device digest the server reports."""
+    from mlmq_tpds_withl3_b200.server import Server, poisson_schedule, serve_poisson, summarize
+    hgs = [HostGraph.grid(1024, 1024, seed=71), HostGraph.grid(256, 256, seed=72),
+           HostGraph.rmat(18, seed=73), HostGraph.rmat(20, seed=74)]
+    dgs = [DeviceGraph.upload(g) for g in hgs]
+    cfg = default_config(delta=100000, warps_per_block=8, relax_unroll=2, l2_cap_log2=20,
+                         l2_batch=16, bucket_max=2)
+    sv = Server(slots=32, max_vertices=max(dg.slots for dg in dgs), cfg=cfg, lifetime_s=300)
+    sched = poisson_schedule(2000.0, 300, [g.n for g in hgs], seed=75)
+    recs = serve_poisson(sv, dgs, sched, keep=lambda i: True, timeout_s=200)
+    sv.close()
+    s = summarize(recs)
+    assert s["errors"] == 0 and s["finished"] == 300
+    by_graph = {}
+    for i, r in enumerate(recs):
+        by_graph.setdefault(r["graph"], []).append(i)
+    for gi, idx in by_graph.items():
+        srcs = [recs[i]["src"] for i in idx]
+        ref, _ = oracle_lib.sssp_many(hgs[gi], srcs)
+        for k, i in enumerate(idx):
+            assert np.array_equal(recs[i]["dist"], ref[k]), (gi, srcs[k])
+            assert recs[i]["digest"] == oracle_lib.digest(ref[k]), (gi, srcs[k])
+    for dg in dgs:
+        dg.close()

@@ -79,6 +79,9 @@ def test_c1_grid512_bit_exact():
     {"relax_unroll": 1, "warps_per_block": 31},
     {"vertex_tiles": 0},
     {"vertex_tiles": 0, "relax_precheck": 0, "relax_unroll": 1},
+    {"vertex_tiles": 2},
+    {"vertex_tiles": 2, "light_heavy": 1, "bucket_sync": 1, "delta": 30000},
+    {"vertex_tiles": 2, "relax_unroll": 1, "large_degree": 4096},
     {"topup": 32},
     {"topup": 16, "l1_ahead": 0, "min_read": 1},
     {"l1_ahead": 1, "delta": 2000},
@@ -130,6 +133,14 @@ def test_split_heavy_vertices_exact():
     # narrow buckets push pieces through L3 as well
     t = Solver(dg, {"bucket_num": 2, "bucket_max": 1, "delta": 3000, "timeout_ms": 15000})
     assert np.array_equal(t.solve(0).dist(), ref[0])
+    # wide tiles (8 inline arcs) with split vertices, single and batched
+    wide = Solver(dg, {"vertex_tiles": 2})
+    for k, src in enumerate(srcs):
+        assert np.array_equal(wide.solve(src).dist(), ref[k]), src
+    bw = BatchSolver(len(srcs), dg.slots, {"vertex_tiles": 2, "topup": 32})
+    bw.run([(dg, x) for x in srcs])
+    for k in range(len(srcs)):
+        assert np.array_equal(bw.dist(k), ref[k])
     # light/heavy split (heavy arcs and heavy pieces one bucket later),
     # single and batched, also through narrow buckets and L3
     for cfg in ({"light_heavy": 1}, {"light_heavy": 1, "delta": 20000, "bucket_sync": 1,

@@ -258,3 +258,31 @@ def test_freeing_while_a_server_runs_does_not_wait_for_it():
     assert done.get(tk) == 0
     sv.close()
     assert np.array_equal(buf.numpy(), oracle_lib.sssp_i32(g, 17)[0])
+
+
+def test_server_with_wide_tiles_needs_them_prepared():
+    """A server reading 64-byte tiles refuses a graph whose wide tiles were
+    not built before it started (nothing is built inside submit); prepared
+    graphs give exact results."""
+    import time
+    import torch
+    from mlmq_tpds_withl3_b200 import MlmqError, default_config
+    from mlmq_tpds_withl3_b200._lib import MLMQ_ERR_STATE
+    g = HostGraph.knn(20000, seed=52)
+    a, b = DeviceGraph.upload(g), DeviceGraph.upload(g)
+    a.prepare_tiles(2)
+    sv = Server(slots=2, max_vertices=g.n, cfg=default_config(warps_per_block=8, vertex_tiles=2),
+                lifetime_s=60)
+    buf = torch.empty(g.n, dtype=torch.int32, pin_memory=True)
+    with pytest.raises(MlmqError) as ei:
+        sv.submit(b, 0, buf)
+    assert ei.value.code == MLMQ_ERR_STATE
+    del ei
+    tk = sv.submit(a, 11, buf)
+    done = {}
+    t = time.time()
+    while tk not in done and time.time() - t < 20:
+        done.update(dict(sv.poll()))
+    sv.close()
+    assert done.get(tk) == 0
+    assert np.array_equal(buf.numpy(), oracle_lib.sssp_i32(g, 11)[0])

@@ -146,3 +146,35 @@ def test_transform_argument_errors():
         g.chain_shortcuts(source=-1)
     with pytest.raises(MlmqError):
         g.chain_shortcuts(source=0, cut=65)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_gpu_reorder_matches_reference_digest(name):
+    """BFS reordering as a device preprocessing step: the reference tool's
+    output (golden digests made by graph_transform/reorder_gr.cu) byte for
+    byte, for every golden fixture and root."""
+    g, _ = GRAPHS[name]
+    for root, want in GOLD[name]["reorder"].items():
+        r, perm, inv = g.reorder_bfs_gpu(int(root))
+        assert r.m == want["m"]
+        assert digest(r.row, r.col, r.w, perm, inv) == want["sha256"], (name, root)
+
+
+@pytest.mark.gpu
+def test_gpu_reorder_equals_host_on_large_graphs():
+    """Large road-like, kNN and R-MAT graphs (hubs, unreached vertices, many
+    levels): the device reordering equals the host one, and the reordered
+    graph solves to the permuted distances on the GPU."""
+    from mlmq_tpds_withl3_b200 import DeviceGraph, Solver
+    for g, root in ((HostGraph.grid(700, 500, drop_p=0.3, seed=61), 1234),
+                    (HostGraph.knn(300000, seed=62), 77),
+                    (HostGraph.rmat(17, seed=63), 5)):
+        h, hp, hi = g.reorder_bfs(root)
+        d, dp, di = g.reorder_bfs_gpu(root)
+        assert np.array_equal(hp, dp) and np.array_equal(hi, di), g
+        assert np.array_equal(h.row, d.row) and np.array_equal(h.col, d.col)
+        assert np.array_equal(h.w, d.w)
+        ref, _ = oracle_lib.sssp_i32(g, root)
+        got = Solver(DeviceGraph.upload(d)).solve(int(di[root])).dist()
+        assert np.array_equal(got[di], ref), g
