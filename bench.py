@@ -11,8 +11,8 @@ tuned on other sources) and which carries three more measured blocks:
   "batched"  64 sources on a 4896^2 road-like grid in one persistent launch
              replayed from a CUDA graph, against 64 back-to-back plain solves,
   "served"   continuous batching over 8 HBM-resident graphs under Poisson
-             arrivals (1000/s offered, and a saturating burst), p50/p99
-             latency, against back-to-back plain solves of the same mix.
+             arrivals (100/s and 1000/s offered, and a saturating burst),
+             p50/p99 latency, against back-to-back plain solves of the mix.
 
 Every result of every block is checked against the CPU oracle outside the
 timed regions: plain and batched distances element by element, served
@@ -93,6 +93,10 @@ def parse(argv=None):
                     help="served: queries in each of the two runs")
     ap.add_argument("--burst-rate", type=float, default=20000.0,
                     help="served: arrival rate of the saturating run (queries/s)")
+    ap.add_argument("--light-rate", type=float, default=100.0,
+                    help="served: arrival rate of the light-load run (queries/s)")
+    ap.add_argument("--light-queries", type=int, default=200,
+                    help="served: queries in the light-load run")
     ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--slot-warps", type=int, default=8, help="served: worker warps per CTA")
     ap.add_argument("--sources", type=int, default=0, help="limit the number of sources")
@@ -616,8 +620,12 @@ def served_arm(args, rep, local):
     dgs = [DeviceGraph.upload(hgs[k]) for k in names]
     ns = [hgs[k].n for k in names]
     max_n = max(dg.slots for dg in dgs)
+    # Vertices up to 1024 arcs are spread over the warp's lanes with the
+    # others' arcs instead of being relaxed one at a time by the whole warp
+    # (heavier ones are split into pieces anyway): R-MAT solves ran faster
+    # that way, grids (degree <= 4) do not notice.
     cfg = default_config(delta=100000, warps_per_block=args.slot_warps, relax_unroll=2,
-                         l2_cap_log2=20, l2_batch=16, bucket_max=2)
+                         l2_cap_log2=20, l2_batch=16, bucket_max=2, large_degree=4096)
     knobs = None
     tune_report = None
     if not args.no_tune:
@@ -625,7 +633,8 @@ def served_arm(args, rep, local):
         # a batched launch of 64 of its own queries (sources other than the
         # served ones); the server passes them with every query.
         knobs, tune_report = [], {}
-        base = {**autotune.BATCH_BASE, "warps_per_block": args.slot_warps, "relax_unroll": 2}
+        base = {**autotune.BATCH_BASE, "warps_per_block": args.slot_warps, "relax_unroll": 2,
+                "large_degree": 4096}
         for i, dg in enumerate(dgs):
             rng = np.random.default_rng(70 + i)
             qs = [(dg, int(s)) for s in rng.integers(0, ns[i], 64)]
@@ -644,9 +653,10 @@ def served_arm(args, rep, local):
     scheds = {}
     sampler = ClockSampler(local)
     with sampler:
-        for key, rate, seed in (("offered", args.served_rate, 101),
-                                ("saturation", args.burst_rate, 102)):
-            sched = poisson_schedule(rate, args.served_queries, ns, seed=seed)
+        for key, rate, seed, count in (("light", args.light_rate, 100, args.light_queries),
+                                       ("offered", args.served_rate, 101, args.served_queries),
+                                       ("saturation", args.burst_rate, 102, args.served_queries)):
+            sched = poisson_schedule(rate, count, ns, seed=seed)
             recs = serve_poisson(sv, dgs, sched, pool=pool, timeout_s=600, knobs=knobs)
             runs[key] = recs
             scheds[key] = sched
@@ -712,6 +722,7 @@ def served_arm(args, rep, local):
                 bad += 1
     sat = summarize(runs["saturation"], names)
     off = summarize(runs["offered"], names)
+    light = summarize(runs["light"], names)
     plain_qps = 1e3 / float(np.mean(plain_ms))
     qps = rep.sum(sat["qps"])
     plain_qps = rep.sum(plain_qps)
@@ -721,10 +732,13 @@ def served_arm(args, rep, local):
                    "graphs": {k: {"n": hgs[k].n, "m": hgs[k].m} for k in names},
                    "queries_per_run": args.served_queries,
                    "offered_rate": args.served_rate, "burst_rate": args.burst_rate,
+                   "light_rate": args.light_rate, "light_queries": args.light_queries,
                    **info, "slot_settings": cfg_summary(cfg)},
         "saturation": {k: sat.get(k) for k in ("qps", "p50_ms", "p99_ms", "mean_ms", "finished",
                                                "errors", "error_codes")},
         "offered": {k: off.get(k) for k in ("qps", "p50_ms", "p99_ms", "mean_ms", "finished",
+                                            "errors", "error_codes")},
+        "light": {k: light.get(k) for k in ("qps", "p50_ms", "p99_ms", "mean_ms", "finished",
                                             "errors", "error_codes")},
         "latency_ms": {"p50": off["p50_ms"], "p99": off["p99_ms"],
                        "at_offered_rate": args.served_rate},

@@ -144,7 +144,12 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
                 and on the default one (greedy stages can pick a shape that
                 is wrong with the split);
       claims    L2 claims of 16 slots (they pay with the split on R-MAT and
-                cost narrow-frontier solves)."""
+                cost narrow-frontier solves);
+      refine    relaxation rounds, tile width, warp-cooperative relaxation and
+                the run-ahead bound once more, on top of the split and claim
+                choices.
+
+    A candidate that repeats the current best is not timed again."""
     key = graph_class(hg, kind)
     base = dict(extra or {})
     if use_cache:
@@ -195,6 +200,16 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
             for dl in (shape["delta"], max(1, shape["delta"] // 4)):
                 consider({**shape, "light_heavy": 1, "bucket_sync": 1, "delta": dl})
     consider({**best, "l2_batch": 16})
+    # One refinement pass: the option stages again on top of what the split
+    # and claim stages chose (an option can pay only in combination, e.g.
+    # relaxing hubs through the prefix-sum spread once the split is on).
+    refined = dict(best)
+    for opt in ({"relax_unroll": 1}, {"relax_unroll": 2}, {"relax_unroll": 4},
+                {"vertex_tiles": 0}, {"vertex_tiles": 1}, {"vertex_tiles": 2},
+                {"large_degree": 4096}, {"l1_ahead": 0}):
+        over = {**refined, **opt}
+        if over != best and not (opt.get("vertex_tiles") == 0 and best.get("light_heavy")):
+            consider(over)
     report = {"key": key, "config": best, "seconds": best_t, "trials": results,
               "probe": probe, "adaptive_seed": seed}
     if use_cache:
