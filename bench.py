@@ -335,6 +335,12 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
     world = rep.world
 
     dg = DeviceGraph.upload(g)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush_l2():
+        flush.zero_()
+        torch.cuda.synchronize()
+
     tune_report = None
     if args.config:
         cfg = default_config(**{"delta": 200000, **json.loads(args.config)})
@@ -343,7 +349,8 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
     else:
         pool = workloads.c3_source_pool(g) if name == "c3" else None
         probes = workloads.probe_sources(g, srcs, count=4, pool=pool)
-        cfg, tune_report = autotune.tune(dg, g, probes, kind=name, use_cache=False)
+        cfg, tune_report = autotune.tune(dg, g, probes, kind=name, use_cache=False,
+                                         between=flush_l2)
     solver = Solver(dg, cfg)
 
     # Correctness and per-query work (oracle, untimed): every timed source.
@@ -356,7 +363,6 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
             correct = False
 
     stream = torch.cuda.Stream()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def step(events):
         for s in srcs:
@@ -504,7 +510,10 @@ def batched_arm(args, rep, local):
         pcfg = default_config(delta=200000)
     else:
         probes = workloads.probe_sources(g, srcs, count=4, pool=np.arange(g.n))
-        pcfg, _ = autotune.tune(dg, g, probes, kind="c4-plain", use_cache=False)
+        scratch = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        pcfg, _ = autotune.tune(dg, g, probes, kind="c4-plain", use_cache=False,
+                                between=lambda: (scratch.zero_(), torch.cuda.synchronize()))
+        del scratch
     plain = Solver(dg, pcfg)
     plain_ms, plain_out = [], []
     for s in srcs:
@@ -669,6 +678,12 @@ def served_arm(args, rep, local):
     # its own tuned single-solve configuration; the same queries alone must
     # give the digest they had in the mix.
     sample = runs["saturation"][:96]
+    scratch = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def flush_l2():
+        scratch.zero_()
+        torch.cuda.synchronize()
+
     solvers = {}
     plain_ms, plain_by_graph = [], {}
     alone_same = True
@@ -680,9 +695,10 @@ def served_arm(args, rep, local):
             if not args.no_tune:
                 hg = hgs[names[gi]]
                 served_srcs = [x["src"] for x in sample if x["graph"] == gi]
-                probe = workloads.probe_sources(hg, served_srcs, count=4, pool=np.arange(hg.n))
+                probe = workloads.probe_sources(hg, served_srcs, count=4,
+                                                pool=np.flatnonzero(np.diff(hg.row) > 0))
                 pc, _ = autotune.tune(dgs[gi], hg, probe, kind=f"c5-{names[gi]}",
-                                      use_cache=False)
+                                      use_cache=False, between=flush_l2)
             solvers[gi] = Solver(dgs[gi], pc)
         s = solvers[gi]
         e0 = torch.cuda.Event(enable_timing=True)

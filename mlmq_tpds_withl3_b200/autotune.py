@@ -94,11 +94,15 @@ def delta_candidates(hg, around=200000):
     return sorted(c for c in cands if c <= 4 * around)
 
 
-def _time_solve(solver, src, reps=3):
+def _time_solve(solver, src, reps=3, between=None):
     """Median of `reps` timed solves of one source (host clock around a
-    synchronous solve)."""
+    synchronous solve); `between()`, when given, runs before each one (the
+    bench passes an L2 flush, so candidates are timed as they are measured:
+    with the graph's lines evicted, not left warm by the previous solve)."""
     times = []
     for _ in range(reps):
+        if between is not None:
+            between()
         t0 = time.perf_counter()
         solver.solve(src)
         times.append(time.perf_counter() - t0)
@@ -121,10 +125,11 @@ MARGIN = 0.97
 
 
 def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
-         extra=None):
+         extra=None, between=None):
     """Returns (config, report).  Every candidate is timed on every probe
-    source (median of three solves each; the score is the sum over probes),
-    so pass sources other than the ones to be measured.  Stages, each
+    source (median of three solves each, `between()` before each solve; the
+    score is the sum over probes), so pass sources other than the ones to be
+    measured.  Stages, each
     keeping a candidate only when it is at least 3 % faster than the best so
     far:
 
@@ -163,7 +168,7 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         s = Solver(dgraph, {**base, **over})
         try:
             s.solve(probe[0])  # warm-up
-            t = sum(_time_solve(s, src) for src in probe)
+            t = sum(_time_solve(s, src, between=between) for src in probe)
         finally:
             s.close()
         results.append({"config": over, "seconds": t})

@@ -191,17 +191,13 @@ __global__ void widen_tiles_kernel(const int4 *__restrict__ tiles, const int2 *_
         const int4 t0 = tiles[2 * (size_t)v], t1 = tiles[2 * (size_t)v + 1];
         int4 *o = wide + 4 * (size_t)v;
         if (v < n && t0.x == TILE_CSR && t0.z <= TILE_ARCS_WIDE) {
-            int t[16];
-            for (int i = 0; i < 16; i += 2) {
-                t[i] = -1;
-                t[i + 1] = 0;
+            const int beg = t0.y, deg = t0.z;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int2 a = 2 * q < deg ? arcs[beg + 2 * q] : make_int2(-1, 0);
+                const int2 b = 2 * q + 1 < deg ? arcs[beg + 2 * q + 1] : make_int2(-1, 0);
+                o[q] = make_int4(a.x, a.y, b.x, b.y);
             }
-            for (int i = 0; i < t0.z; i++) {
-                const int2 a = arcs[t0.y + i];
-                t[2 * i] = a.x;
-                t[2 * i + 1] = a.y;
-            }
-            for (int q = 0; q < 4; q++) o[q] = make_int4(t[4 * q], t[4 * q + 1], t[4 * q + 2], t[4 * q + 3]);
         } else {
             o[0] = t0;
             o[1] = (v < n && t0.x >= -1) ? t1 : none;  // inline arcs keep their second half

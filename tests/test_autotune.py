@@ -79,7 +79,7 @@ class _FakeSolver:
 def _tune_with_cost(monkeypatch, tmp_path, cost):
     monkeypatch.setenv("MLMQ_TUNE_CACHE", str(tmp_path / "tune.json"))
     monkeypatch.setattr(autotune, "Solver", _FakeSolver)
-    monkeypatch.setattr(autotune, "_time_solve", lambda s, src, reps=3: cost(s.cfg))
+    monkeypatch.setattr(autotune, "_time_solve", lambda s, src, reps=3, between=None: cost(s.cfg))
     monkeypatch.setattr(autotune, "_sm_count", lambda: 148)
     g = HostGraph.grid(32, 32, seed=9)
     return autotune.tune(None, g, [0, 1], kind="fake", use_cache=False)
