@@ -347,10 +347,14 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
     elif name == "c1" or args.no_tune:
         cfg = default_config(delta=200000)
     else:
-        pool = workloads.c3_source_pool(g) if name == "c3" else None
-        probes = workloads.probe_sources(g, srcs, count=4, pool=pool)
-        cfg, tune_report = autotune.tune(dg, g, probes, kind=name, use_cache=False,
-                                         between=flush_l2)
+        # Rank 0 tunes; every replica then runs its configuration.
+        if rep.rank == 0:
+            pool = workloads.c3_source_pool(g) if name == "c3" else None
+            probes = workloads.probe_sources(g, srcs, count=4, pool=pool)
+            cfg, tune_report = autotune.tune(dg, g, probes, kind=name, use_cache=False,
+                                             between=flush_l2)
+        picked = rep.broadcast(cfg.as_dict() if rep.rank == 0 else None)
+        cfg = default_config(**picked)
     solver = Solver(dg, cfg)
 
     # Correctness and per-query work (oracle, untimed): every timed source.
@@ -412,13 +416,16 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
         src_arr = np.asarray(srcs, np.int32)
         out = torch.empty((len(srcs), g.n), dtype=torch.int32).pin_memory()
         e2e_steps = max(1, min(steps, 5))
+        # Warm-up calls as for the device timing: the first calls after tuning
+        # grow the library's memory pool to the call's working set.
+        e2e_warm = max(2, min(warmup, 3))
         walls = []
-        for i in range(e2e_steps + 1):
+        for i in range(e2e_steps + e2e_warm):
             t0 = time.perf_counter()
             check(lib.mlmq_solve_host(g.n, g.m, row.data_ptr(), col.data_ptr(), w.data_ptr(),
                                       len(srcs), src_arr.ctypes.data, out.data_ptr(), cfg),
                   "mlmq_solve_host")
-            if i:
+            if i >= e2e_warm:
                 walls.append(time.perf_counter() - t0)
         e2e_s = rep.max(float(np.sum(walls)))
         correct = correct and np.array_equal(out.numpy(), dists)
@@ -428,6 +435,7 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
                "d2h_bytes_per_step": int(4 * g.n * len(srcs)),
                "ms_per_step": e2e_s / len(walls) * 1e3,
                "walls_ms": [round(x * 1e3, 2) for x in walls],
+               "warmup_calls": e2e_warm,
                "api": "mlmq_solve_host (pinned host CSR in, distances out)"}
         del out, row, col, w
     del dists

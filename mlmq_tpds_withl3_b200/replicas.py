@@ -47,6 +47,17 @@ class Replicas:
             return float(value)
         return self._reduce(value, self._dist.ReduceOp.SUM)
 
+    def broadcast(self, obj):
+        """Rank 0's `obj` (any picklable value) on every rank: the solver
+        configuration rank 0 tuned, so that every replica runs the same one
+        (tuned independently, timing noise could give the ranks different
+        picks and the slowest pick would set the job's time)."""
+        if self._dist is None:
+            return obj
+        box = [obj if self.rank == 0 else None]
+        self._dist.broadcast_object_list(box, src=0)
+        return box[0]
+
     def barrier(self):
         if self._dist is not None:
             self._dist.barrier()

@@ -27,8 +27,9 @@ def _rank_main(rank, world, port, out):
     slowest = rep.max(1.5 + rank)        # rank 1 is the slow one
     total = rep.sum(10.0 * (rank + 1))
     rate = whole_job_rate(100, rep.world, slowest)
+    cfg = rep.broadcast({"delta": 50000, "warps_per_block": 8} if rank == 0 else {"delta": -1})
     rep.close()
-    out.put((rank, rep.world, slowest, total, rate))
+    out.put((rank, rep.world, slowest, total, rate, cfg))
 
 
 def _run(world):
@@ -48,11 +49,12 @@ def _run(world):
 def test_two_ranks_agree_on_max_and_sum():
     res = _run(2)
     assert [r[0] for r in res] == [0, 1]
-    for _, world, slowest, total, rate in res:
+    for _, world, slowest, total, rate, cfg in res:
         assert world == 2
         assert slowest == 2.5
         assert total == 30.0
         assert rate == pytest.approx(2 * 100 / 2.5)
+        assert cfg == {"delta": 50000, "warps_per_block": 8}  # rank 0's tuned configuration
 
 
 def test_single_process_needs_no_process_group(monkeypatch):
