@@ -474,9 +474,12 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
                                                          "l3_pushed", "batches", "idle")},
     }
     if tune_report:
+        trials = sorted(tune_report.get("trials", []), key=lambda t: t["seconds"])
         out["autotune"] = {"config": tune_report.get("config"),
                            "probe_sources": tune_report.get("probe"),
-                           "trials": len(tune_report.get("trials", []))}
+                           "trials": len(trials),
+                           "fastest": [{"config": t["config"], "ms": round(t["seconds"] * 1e3, 2)}
+                                       for t in trials[:4]]}
     return out
 
 

@@ -203,7 +203,15 @@ def tune(dgraph, hg, probe_sources, kind="graph", around=200000, use_cache=True,
         shapes = [best, {"delta": best["delta"]}]
         for shape in shapes[:1] if shapes[0] == shapes[1] else shapes:
             for dl in (shape["delta"], max(1, shape["delta"] // 4)):
-                consider({**shape, "light_heavy": 1, "bucket_sync": 1, "delta": dl})
+                split = {**shape, "light_heavy": 1, "bucket_sync": 1, "delta": dl}
+                if split.get("queue_type") == MLMQ_L1V_L2DQ:
+                    split.pop("queue_type")  # the split is built for the SLF L1
+                # Alone and with the settings it pays with on power-law
+                # graphs (16-slot claims; hubs spread over the lanes): tried
+                # one at a time after this stage, neither would be picked
+                # without the other.
+                consider(split)
+                consider({**split, "l2_batch": 16, "large_degree": 4096})
     consider({**best, "l2_batch": 16})
     # One refinement pass: the option stages again on top of what the split
     # and claim stages chose (an option can pay only in combination, e.g.
