@@ -355,6 +355,8 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
                                              between=flush_l2)
         picked = rep.broadcast(cfg.as_dict() if rep.rank == 0 else None)
         cfg = default_config(**picked)
+        # Tuning leaves the pool holding blocks of every candidate's sizes.
+        lib.mlmq_release_cached()
     solver = Solver(dg, cfg)
 
     # Correctness and per-query work (oracle, untimed): every timed source.
@@ -408,9 +410,11 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
     stats = solver.stats()
     solver.close()
 
-    # End to end through the host-buffer API.
+    # End to end through the host-buffer API (the pool starts from what the
+    # call itself needs; warm-up calls grow it).
     e2e = None
     if e2e_on:
+        lib.mlmq_release_cached()
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
         row, col, w = pin(g.row), pin(g.col), pin(g.w)
         src_arr = np.asarray(srcs, np.int32)

@@ -40,6 +40,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
         }
         const unsigned first = ld_relaxed(p.ctlw + ctl::FIRST);
         const unsigned pres = ld_relaxed(p.ctlw + ctl::PRESSURE);
+        const unsigned upres = ld_relaxed(p.ctlw + ctl::U_PRESSURE);
         const unsigned l3r = ld_relaxed(p.ctlw + ctl::L3_RESERVE);
         const unsigned l3c = ld_relaxed(p.ctlw + ctl::L3_CLAIM);
         const unsigned l3k = ld_relaxed(p.ctlw + ctl::L3_CONSUMED);
@@ -53,6 +54,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
         if (lane == 0) {
             mir.first = first;
             mir.pressure = pres;
+            mir.u_pressure = upres;
             mir.l3_reserve = l3r;
             mir.l3_claim = l3c;
             mir.l3_consumed = l3k;
@@ -209,8 +211,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
 template <class Arcs, int K>
 __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank, unsigned gsize) {
     extern __shared__ uint2 smem[];
-    __shared__ Mirror mir_storage;
-    volatile Mirror &mir = mir_storage;
+    volatile Mirror &mir = cta_mirror;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const unsigned long long deadline = globaltimer() + p.timeout_ns;
@@ -244,6 +245,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         mir.first = 0u;
         mir.exit = 0u;
         mir.pressure = 0u;
+        mir.u_pressure = 0u;
         mir.l3_reserve = mir.l3_claim = mir.l3_consumed = mir.l3_epoch = 0u;
     }
     __syncthreads();
