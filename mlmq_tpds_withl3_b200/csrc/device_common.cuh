@@ -32,7 +32,11 @@ constexpr int OUTBOX_CAP = 64;
 constexpr int OUTBOX_OFF = L1_CAP + 32 + 32 * TILE_ARCS_WIDE;
 constexpr int WINBUF_CAP = 128;
 constexpr int WINBUF_OFF = OUTBOX_OFF + OUTBOX_CAP;
-constexpr int WARP_SMEM_SLOTS = WINBUF_OFF + WINBUF_CAP;
+// Per-warp counters (u64) for kernels that keep them out of registers.
+constexpr int WSTAT_OFF = WINBUF_OFF + WINBUF_CAP;
+constexpr int WS_PUSHED = 0, WS_L3_PUSHED = 1, WS_RELAXED = 2, WS_IMPROVED = 3, WS_BATCHES = 4,
+              WS_IDLE = 5, WS_RANGE = 6, WS_DEADLINE = 7;
+constexpr int WARP_SMEM_SLOTS = WSTAT_OFF + 8;
 
 // ---- control block: 32-bit words, one 128-byte line per group ------------
 namespace ctl {

@@ -18,6 +18,8 @@
 #include "mlmq_b200.h"
 #include "solver_internal.h"
 #include "sssp_plain.h"
+// Per-warp counters in shared memory (see mlmq_queue.cuh).
+#define MLMQ_WARP_STATS_SMEM 1
 #include "sssp_plain_body.cuh"
 
 #include <algorithm>
@@ -47,32 +49,38 @@ struct BatchParams {
     int nq;
 };
 
-// Batched slots use few warps per CTA, so every variant gets the register
-// budget of PLAIN_MAX_THREADS threads.
 template <int K>
-__global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_batch_kernel(BatchParams bp) {
+__global__ void __maxnreg__(SLOT_KERNEL_REGS) sssp_batch_kernel(BatchParams bp) {
     const unsigned g = gridDim.x;
     const unsigned nq = (unsigned)bp.nq;
     const unsigned s = (unsigned)(((unsigned long long)blockIdx.x * nq) / g);
     // First CTA of slot s: ceil(s * g / nq).
     const unsigned lo = (unsigned)(((unsigned long long)s * g + nq - 1) / nq);
     const unsigned hi = (unsigned)(((unsigned long long)(s + 1) * g + nq - 1) / nq);
-    PlainParams p = bp.base;
-    const BatchQuery qy = bp.queries[s];
-    p.row = qy.row;
-    p.arcs = qy.arcs;
-    p.tiles = qy.tiles;
-    p.n = qy.n;
-    p.nslots = qy.nslots;
-    p.nids = qy.nids;
-    p.split = qy.split;
-    p.src = qy.src;
-    p.dist = bp.base.dist + s * bp.dist_stride;
-    p.l2 = bp.base.l2 + s * bp.l2_stride;
-    p.l3 = bp.base.l3 + s * bp.l3_stride;
-    p.l3bits = bp.base.l3bits + s * bp.bits_stride;
-    p.ctlw = bp.base.ctlw + s * bp.ctl_stride;
-    plain_body<ArcsInterleaved, K>(p, blockIdx.x - lo, hi - lo);
+    // The slot's parameters go to shared memory, not registers: the solve
+    // reads them from there (or the constant bank), which keeps the kernel
+    // at 56 registers, four CTAs of nine warps per SM.
+    __shared__ PlainParams cta_params;
+    if (threadIdx.x == 0) {
+        PlainParams p = bp.base;
+        const BatchQuery qy = bp.queries[s];
+        p.row = qy.row;
+        p.arcs = qy.arcs;
+        p.tiles = qy.tiles;
+        p.n = qy.n;
+        p.nslots = qy.nslots;
+        p.nids = qy.nids;
+        p.split = qy.split;
+        p.src = qy.src;
+        p.dist = bp.base.dist + s * bp.dist_stride;
+        p.l2 = bp.base.l2 + s * bp.l2_stride;
+        p.l3 = bp.base.l3 + s * bp.l3_stride;
+        p.l3bits = bp.base.l3bits + s * bp.bits_stride;
+        p.ctlw = bp.base.ctlw + s * bp.ctl_stride;
+        cta_params = p;
+    }
+    __syncthreads();
+    plain_body<ArcsInterleaved, K>(cta_params, blockIdx.x - lo, hi - lo);
 }
 
 const void *batch_kernel(int unroll) {

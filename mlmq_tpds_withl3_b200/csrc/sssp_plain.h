@@ -12,6 +12,11 @@ struct PlainParams;
 // relaxation round in flight (24 worker warps + the manager): their register
 // budget is sized for it.
 constexpr int PLAIN_MAX_THREADS = 800;
+// Register cap of the batched and served kernels: 56 registers fit four CTAs
+// of nine warps on an SM (three at the 64-72 registers they would take
+// uncapped), and with their counters and per-query parameters in shared
+// memory they do not spill at it.
+constexpr int SLOT_KERNEL_REGS = 56;
 
 // Dynamic shared memory of one CTA with `workers` worker warps.
 size_t plain_smem_bytes(int workers);

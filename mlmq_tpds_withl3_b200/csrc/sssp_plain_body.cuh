@@ -184,7 +184,8 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
                     continue;
                 }
 
-                q.idle++;
+                if constexpr (kStatsSmem) wstat_add(WS_IDLE, 1u);
+                else q.idle++;
                 __nanosleep(q.idle_ns);
                 if (q.idle_ns < 256) q.idle_ns <<= 1;
                 continue;
@@ -200,7 +201,8 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
             }
             __syncwarp();
         }
-        q.batches++;
+        if constexpr (kStatsSmem) wstat_add(WS_BATCHES, 1u);
+        else q.batches++;
         relax_batch<Arcs, K>(p, q, ring, stage, valid, v, d);
     }
 }
@@ -270,25 +272,48 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
     q.pushed = q.l3_pushed = q.relaxed = q.improved = 0ull;
     q.batches = q.idle = 0u;
     q.deadline = deadline;
+    if constexpr (kStatsSmem) {
+        if (lane < 8) wstat()[lane] = lane == WS_DEADLINE ? deadline : 0ull;
+        __syncwarp();
+    }
 
     worker_loop<Arcs, K>(p, mir, ring, inb, stage, q);
 
     // ---- epilogue: statistics --------------------------------------------------
-    unsigned long long relaxed = q.relaxed, improved = q.improved;
+    unsigned long long pushed, l3_pushed, relaxed, improved, batches, idle;
+    bool range;
+    if constexpr (kStatsSmem) {
+        __syncwarp();
+        const unsigned long long *ws = wstat();
+        pushed = ws[WS_PUSHED];
+        l3_pushed = ws[WS_L3_PUSHED];
+        relaxed = ws[WS_RELAXED];
+        improved = ws[WS_IMPROVED];
+        batches = ws[WS_BATCHES];
+        idle = ws[WS_IDLE];
+        range = ws[WS_RANGE] != 0ull;
+    } else {
+        pushed = q.pushed;
+        l3_pushed = q.l3_pushed;
+        relaxed = q.relaxed;
+        improved = q.improved;
+        batches = q.batches;
+        idle = q.idle;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        relaxed += __shfl_xor_sync(FULL, relaxed, o);
-        improved += __shfl_xor_sync(FULL, improved, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            relaxed += __shfl_xor_sync(FULL, relaxed, o);
+            improved += __shfl_xor_sync(FULL, improved, o);
+        }
+        range = __ballot_sync(FULL, q.range_hit != 0u) != 0u;
     }
-    const unsigned range = __ballot_sync(FULL, q.range_hit != 0u);
     if (lane == 0) {
         unsigned long long *st = reinterpret_cast<unsigned long long *>(p.ctlw + ctl::STATS);
-        atomicAdd(st + ctl::ST_PUSHED, q.pushed);
-        atomicAdd(st + ctl::ST_L3_PUSHED, q.l3_pushed);
+        atomicAdd(st + ctl::ST_PUSHED, pushed);
+        atomicAdd(st + ctl::ST_L3_PUSHED, l3_pushed);
         atomicAdd(st + ctl::ST_RELAXED, relaxed);
         atomicAdd(st + ctl::ST_IMPROVED, improved);
-        atomicAdd(st + ctl::ST_BATCHES, (unsigned long long)q.batches);
-        atomicAdd(st + ctl::ST_IDLE, (unsigned long long)q.idle);
+        atomicAdd(st + ctl::ST_BATCHES, batches);
+        atomicAdd(st + ctl::ST_IDLE, idle);
         if (range) atomicOr(p.ctlw + ctl::STATUS, ST_RANGE);
         atomicMax(st + ctl::ST_FIRST_MAX, (unsigned long long)ld_relaxed(p.ctlw + ctl::FIRST));
     }

@@ -29,6 +29,8 @@
 #include "mlmq_b200.h"
 #include "solver_internal.h"
 #include "sssp_plain.h"
+// Per-warp counters in shared memory (see mlmq_queue.cuh).
+#define MLMQ_WARP_STATS_SMEM 1
 #include "sssp_plain_body.cuh"
 
 #include <algorithm>
@@ -148,25 +150,39 @@ __device__ bool group_barrier(unsigned *c, unsigned gsize, unsigned long long de
     return ok != 0;
 }
 
-// Server slots use few warps per CTA, so every variant gets the register
-// budget of PLAIN_MAX_THREADS threads.
 template <int K>
-__global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(ServerParams sp) {
+__global__ void __maxnreg__(SLOT_KERNEL_REGS) sssp_server_kernel(ServerParams sp) {
     // Slot s is the CTA group [slot_first[s], slot_first[s + 1]); slots may
     // differ in size (small ones for latency-bound queries, wide ones for
     // throughput-bound queries).
-    const unsigned s = (unsigned)sp.cta_slot[blockIdx.x];
-    const unsigned lo = (unsigned)sp.slot_first[s];
-    const unsigned hi = (unsigned)sp.slot_first[s + 1];
-    const unsigned grank = blockIdx.x - lo, gsize = hi - lo;
-    unsigned *c = sp.ctl + (size_t)s * SRV_CTL_STRIDE;
-    const unsigned long long end = globaltimer() + sp.lifetime_ns;
+    // The slot's identity and the loop's state live in shared memory, not in
+    // registers that would stay allocated through every solve.
+    struct SlotState {
+        unsigned long long end, seen, t_go;
+        unsigned *c;
+        unsigned s, grank, gsize;
+    };
+    __shared__ SlotState ss;
     __shared__ unsigned long long go_seq, go_time;
     __shared__ int stop;
-    unsigned long long seen = 0;
+    if (threadIdx.x == 0) {
+        const unsigned s = (unsigned)sp.cta_slot[blockIdx.x];
+        const unsigned lo = (unsigned)sp.slot_first[s];
+        const unsigned hi = (unsigned)sp.slot_first[s + 1];
+        ss.s = s;
+        ss.grank = blockIdx.x - lo;
+        ss.gsize = hi - lo;
+        ss.c = sp.ctl + (size_t)s * SRV_CTL_STRIDE;
+        ss.end = globaltimer() + sp.lifetime_ns;
+        ss.seen = 0;
+    }
+    __syncthreads();
     for (;;) {
         // ---- wait for the slot's next command ------------------------------
         if (threadIdx.x == 0) {
+            const unsigned s = ss.s, grank = ss.grank;
+            unsigned *c = ss.c;
+            const unsigned long long end = ss.end, seen = ss.seen;
             stop = 0;
             unsigned ns = 256;
             for (;;) {
@@ -240,39 +256,52 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
         }
         __syncthreads();
         if (stop) return;
-        seen = go_seq;
-        // This CTA's view of when the query started: its solve ends by this
-        // plus the query's time limit.
-        const unsigned long long t_go = globaltimer();
         // ---- one solve --------------------------------------------------------
-        PlainParams p = sp.base;
-        const volatile unsigned *cmd = c + SRV_CMD;
-        p.row = (const int *)(((unsigned long long)cmd[1] << 32) | cmd[0]);
-        p.arcs = (const int2 *)(((unsigned long long)cmd[3] << 32) | cmd[2]);
-        p.tiles = (const int4 *)(((unsigned long long)cmd[7] << 32) | cmd[6]);
-        p.delta = cmd[8];
-        p.topup = (int)cmd[9];
-        p.l1_ahead = (int)cmd[10];
-        p.bm = (int)cmd[11];
-        p.nslots = (int)cmd[12];
-        p.bucket_sync = (int)cmd[13];
-        p.nids = (int)cmd[14];
-        p.split = (const int *)(((unsigned long long)cmd[16] << 32) | cmd[15]);
-        p.n = (int)cmd[4];
-        p.src = (int)cmd[5];
-        p.dist = sp.dist + (size_t)s * sp.max_n;
-        p.l2 = sp.l2 + ((size_t)s * (p.nb + 1) << p.l2_log);
-        p.l3 = sp.l3 + ((size_t)s << p.l3_log);
-        p.l3bits = sp.l3bits + (size_t)s * sp.bits_words;
-        p.ctlw = c;
-        plain_body<ArcsInterleaved, K>(p, grank, gsize);
+        // The query's parameters go to shared memory, not registers (as in
+        // the batched kernel).  Every thread has passed the __syncthreads
+        // above since the last read of the previous query's copy.
+        __shared__ PlainParams cta_params;
+        if (threadIdx.x == 0) {
+            const unsigned s = ss.s;
+            unsigned *c = ss.c;
+            ss.seen = go_seq;
+            // This CTA's view of when the query started: its solve ends by
+            // this plus the query's time limit.
+            ss.t_go = globaltimer();
+            PlainParams p = sp.base;
+            const volatile unsigned *cmd = c + SRV_CMD;
+            p.row = (const int *)(((unsigned long long)cmd[1] << 32) | cmd[0]);
+            p.arcs = (const int2 *)(((unsigned long long)cmd[3] << 32) | cmd[2]);
+            p.tiles = (const int4 *)(((unsigned long long)cmd[7] << 32) | cmd[6]);
+            p.delta = cmd[8];
+            p.topup = (int)cmd[9];
+            p.l1_ahead = (int)cmd[10];
+            p.bm = (int)cmd[11];
+            p.nslots = (int)cmd[12];
+            p.bucket_sync = (int)cmd[13];
+            p.nids = (int)cmd[14];
+            p.split = (const int *)(((unsigned long long)cmd[16] << 32) | cmd[15]);
+            p.n = (int)cmd[4];
+            p.src = (int)cmd[5];
+            p.dist = sp.dist + (size_t)s * sp.max_n;
+            p.l2 = sp.l2 + ((size_t)s * (p.nb + 1) << p.l2_log);
+            p.l3 = sp.l3 + ((size_t)s << p.l3_log);
+            p.l3bits = sp.l3bits + (size_t)s * sp.bits_words;
+            p.ctlw = c;
+            cta_params = p;
+        }
+        __syncthreads();
+        const PlainParams &p = cta_params;
+        plain_body<ArcsInterleaved, K>(p, ss.grank, ss.gsize);
+        const unsigned s = ss.s, grank = ss.grank, gsize = ss.gsize;
+        unsigned *c = ss.c;
         if ((int)blockIdx.x == sp.absent_cta) return;  // test: a CTA that never arrives
         // Every CTA of the slot leaves the solve before anything else: after
         // this barrier nothing writes the status word any more, so every CTA
         // reads the same final status (read before it, a CTA could miss a
         // bit that a slower CTA still sets, and the CTAs would then take
         // different barriers below).  Bounded by the query's own limit.
-        bool ok = group_barrier(c, gsize, t_go + p.timeout_ns + sp.meet_ns);
+        bool ok = group_barrier(c, gsize, ss.t_go + p.timeout_ns + sp.meet_ns);
         __shared__ unsigned solve_status;
         if (threadIdx.x == 0) solve_status = ld_acquire(c + ctl::STATUS);
         __syncthreads();
@@ -323,7 +352,7 @@ __global__ void __launch_bounds__(PLAIN_MAX_THREADS, 1) sssp_server_kernel(Serve
             sp.done[s].t_start = go_time;
             sp.done[s].t_end = globaltimer();
             __threadfence_system();
-            sp.done[s].seq = seen;
+            sp.done[s].seq = ss.seen;
             __threadfence_system();
         }
         if (!ok) return;
