@@ -163,16 +163,20 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
             }
         } else {
             if (q.ob_n) outbox_flush(p, q, ring, true);
-            if (q.onfly) {
-                // L1 and the outbox are empty: everything derived from the
-                // records read so far is reserved in L2/L3, so their credit
-                // may go back.
+            int got = l2_has_work(p, q, mir) ? l2_read(p, q, mir, inb, 32, p.min_read) : 0;
+            if (got == 0 && q.onfly) {
+                // L1 and the outbox are empty and L2 has nothing for this
+                // warp: everything derived from the records read so far is
+                // reserved in L2/L3, so their credit may go back.  A warp
+                // that finds more records keeps its credit and returns it
+                // with theirs, which takes the fence off the busy path
+                // (R-MAT-22 +3 %); a warp always reads L2 before it idles,
+                // so credit is never held by an idle warp.
                 __threadfence();
                 __syncwarp();
                 if (lane == 0) atomicAdd(p.ctlw + ctl::CREDIT, q.onfly);
                 q.onfly = 0;
             }
-            int got = l2_has_work(p, q, mir) ? l2_read(p, q, mir, inb, 32, p.min_read) : 0;
             if (got == 0) {
                 // Nothing in L2: re-bucket L3 records if an epoch is open.
                 // Their credit is returned once L1 is empty, after the
