@@ -254,6 +254,11 @@ int mlmq_graph_prepare_light(const mlmq_graph *g, int delta);
  * first use, a server cannot (as for mlmq_graph_prepare_light): prepare
  * before the server starts. */
 int mlmq_graph_prepare_tiles(const mlmq_graph *g, int vertex_tiles);
+/* Copies the graph's arcs, in the order the kernels read them (each vertex's
+ * arcs a permutation of its input arcs, sorted by weight), into host arrays
+ * of m ints: col[e] destination, w[e] weight.  Synchronous; for inspection
+ * and tests. */
+int mlmq_graph_copy_arcs(const mlmq_graph *g, int *col, int *w);
 void mlmq_graph_free(mlmq_graph *g);
 
 /* A solver owns one distance array and one queue workspace on the device

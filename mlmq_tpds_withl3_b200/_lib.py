@@ -115,6 +115,7 @@ _sig("mlmq_graph_upload", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(
 _sig("mlmq_graph_wrap_device", c_int, c_int, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_vp))
 _sig("mlmq_graph_size", c_int, c_vp, ctypes.POINTER(c_int), ctypes.POINTER(c_i64))
 _sig("mlmq_graph_pieces", c_int, c_vp, ctypes.POINTER(c_int))
+_sig("mlmq_graph_copy_arcs", c_int, c_vp, c_vp, c_vp)
 _sig("mlmq_graph_prepare_light", c_int, c_vp, c_int)
 _sig("mlmq_graph_prepare_tiles", c_int, c_vp, c_int)
 _sig("mlmq_graph_free", None, c_vp)

@@ -61,6 +61,15 @@ class DeviceGraph:
         to 8 inline arcs), needed before a server with that setting starts."""
         check(lib.mlmq_graph_prepare_tiles(self._h, int(vertex_tiles)), "mlmq_graph_prepare_tiles")
 
+    def arcs(self):
+        """(col, w): the arcs in the order the kernels read them -- each
+        vertex's arcs a permutation of its input arcs, sorted by weight."""
+        col = np.empty(self.m, np.int32)
+        w = np.empty(self.m, np.int32)
+        check(lib.mlmq_graph_copy_arcs(self._h, col.ctypes.data, w.ctypes.data),
+              "mlmq_graph_copy_arcs")
+        return col, w
+
     def close(self):
         if self._h is not None and self._h.value:
             lib.mlmq_graph_free(self._h)
