@@ -419,7 +419,7 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
         row, col, w = pin(g.row), pin(g.col), pin(g.w)
         src_arr = np.asarray(srcs, np.int32)
         out = torch.empty((len(srcs), g.n), dtype=torch.int32).pin_memory()
-        e2e_steps = max(1, min(steps, 5))
+        e2e_steps = max(3, min(steps, 9))
         # Warm-up calls as for the device timing: the first calls after tuning
         # grow the library's memory pool to the call's working set and load
         # the upload's sort kernels (R-MAT-22: the first calls took 90-650 ms
@@ -434,13 +434,20 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
                   "mlmq_solve_host")
             if i >= e2e_warm:
                 walls.append(time.perf_counter() - t0)
-        e2e_s = rep.max(float(np.sum(walls)))
+        # The median step: the PCIe link and the host are shared with the
+        # machine's other GPUs and their jobs, and single calls now and then
+        # take 2-10x longer for it (every wall is listed, with the mean).
+        e2e_s = rep.max(float(np.median(walls)))
+        e2e_mean = rep.max(float(np.mean(walls)))
         correct = correct and np.array_equal(out.numpy(), dists)
-        e2e = {"value": whole_job_rate(work_step * len(walls), world, e2e_s) / 1e9,
+        e2e = {"value": whole_job_rate(work_step, world, e2e_s) / 1e9,
                "unit": "GTEPS",
                "h2d_bytes_per_step": int(4 * (g.n + 1) + 8 * g.m),
                "d2h_bytes_per_step": int(4 * g.n * len(srcs)),
-               "ms_per_step": e2e_s / len(walls) * 1e3,
+               "ms_per_step": e2e_s * 1e3,
+               "statistic": "median of the steps",
+               "mean_ms_per_step": e2e_mean * 1e3,
+               "value_from_mean": whole_job_rate(work_step, world, e2e_mean) / 1e9,
                "walls_ms": [round(x * 1e3, 2) for x in walls],
                "warmup_calls": e2e_warm,
                "api": "mlmq_solve_host (pinned host CSR in, distances out)"}

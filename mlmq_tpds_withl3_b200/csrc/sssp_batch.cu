@@ -49,7 +49,9 @@ struct BatchParams {
     int nq;
 };
 
-template <int K>
+// kSplit as for the single-solve kernel: true when a query's graph has
+// pieces or the batch runs the light/heavy split.
+template <int K, bool kSplit>
 __global__ void __maxnreg__(SLOT_KERNEL_REGS) sssp_batch_kernel(BatchParams bp) {
     const unsigned g = gridDim.x;
     const unsigned nq = (unsigned)bp.nq;
@@ -80,14 +82,14 @@ __global__ void __maxnreg__(SLOT_KERNEL_REGS) sssp_batch_kernel(BatchParams bp) 
         cta_params = p;
     }
     __syncthreads();
-    plain_body<ArcsInterleaved, K>(cta_params, blockIdx.x - lo, hi - lo);
+    plain_body<ArcsInterleaved, K, kSplit>(cta_params, blockIdx.x - lo, hi - lo);
 }
 
-const void *batch_kernel(int unroll) {
+const void *batch_kernel(int unroll, bool split) {
     switch (unroll) {
-        case 1: return (const void *)sssp_batch_kernel<1>;
-        case 2: return (const void *)sssp_batch_kernel<2>;
-        default: return (const void *)sssp_batch_kernel<4>;
+        case 1: return split ? (const void *)sssp_batch_kernel<1, true> : (const void *)sssp_batch_kernel<1, false>;
+        case 2: return split ? (const void *)sssp_batch_kernel<2, true> : (const void *)sssp_batch_kernel<2, false>;
+        default: return split ? (const void *)sssp_batch_kernel<4, true> : (const void *)sssp_batch_kernel<4, false>;
     }
 }
 
@@ -115,6 +117,7 @@ struct mlmq_batch {
     int nq = 0;
     std::vector<int> n_of;            // vertex count per active slot
     cudaGraphExec_t exec = nullptr;   // captured launch of the current query set
+    bool split = true;                // launch the split-capable kernel variant
     std::vector<long long> exec_key;  // (graph pointer, src) per slot of `exec`
     bool graph_cooperative = true;
     // Graphs referenced by the last launch and by `exec` (one reference
@@ -189,7 +192,7 @@ int enqueue(mlmq_batch *b, int nq, cudaStream_t st) {
     bp.ctl_stride = CTL_STRIDE;
     bp.nq = nq;
     void *args[] = {&bp};
-    rc = cuda_fail(cudaLaunchKernelExC(&lc, batch_kernel(b->cfg.relax_unroll), args),
+    rc = cuda_fail(cudaLaunchKernelExC(&lc, batch_kernel(b->cfg.relax_unroll, b->split), args),
                    "batch launch");
     if (rc) return rc;
     return cuda_fail(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(unsigned) * CTL_STRIDE * nq,
@@ -226,12 +229,17 @@ extern "C" int mlmq_batch_create(int max_queries, int max_vertices, const mlmq_c
     if (!rc) {
         const int threads = 32 * (b->workers + 1);
         const size_t smem = plain_smem_bytes(b->workers);
-        const void *k = batch_kernel(cfg.relax_unroll);
-        rc = cuda_fail(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)plain_smem_limit()), "batch smem");
-        if (!rc)
-            rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem),
-                           "batch occupancy");
+        // The smaller occupancy of the two variants (either may run on the grid).
+        for (int split = 0; split < 2 && !rc; split++) {
+            const void *k = batch_kernel(cfg.relax_unroll, split != 0);
+            rc = cuda_fail(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)plain_smem_limit()), "batch smem");
+            int bk = 0;
+            if (!rc)
+                rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bk, k, threads, smem),
+                               "batch occupancy");
+            bps = split ? std::min(bps, bk) : bk;
+        }
     }
     if (!rc) {
         const int maxgrid = bps * sms;
@@ -302,7 +310,13 @@ extern "C" int mlmq_batch_run(mlmq_batch *b, int nq, const mlmq_graph *const *gr
     for (const mlmq_graph *g : b->held) graph_release(g);
     b->held.swap(hold);
     std::vector<long long> key;
-    key.reserve(2 * (size_t)nq);
+    key.reserve(2 * (size_t)nq + 1);
+    // The kernel variant is part of a captured launch: the split-capable one
+    // when a graph has pieces or the light/heavy split is on.
+    b->split = b->cfg.light_heavy != 0;
+    for (int q = 0; q < nq; q++)
+        if (graphs[q]->pieces > 0) b->split = true;
+    key.push_back(b->split ? 1 : 0);
     b->n_of.assign((size_t)nq, 0);
     for (int q = 0; q < nq; q++) {
         const mlmq_graph *g = graphs[q];

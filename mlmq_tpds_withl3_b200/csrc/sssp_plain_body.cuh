@@ -129,7 +129,7 @@ __device__ __forceinline__ void manager_loop(const PlainParams &p, volatile Mirr
     }
 }
 
-template <class Arcs, int K>
+template <class Arcs, int K, bool kSplit>
 __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirror &mir, uint2 *ring,
                                             uint2 *inb, int2 *stage, WarpQ &q) {
     const int lane = threadIdx.x & 31;
@@ -181,7 +181,7 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
                 // Nothing in L2: re-bucket L3 records if an epoch is open.
                 // Their credit is returned once L1 is empty, after the
                 // pushes that re-bucketed them.
-                const int moved = l3_rebucket(p, q, mir);
+                const int moved = l3_rebucket<kSplit>(p, q, mir);
                 if (moved) {
                     q.onfly += (unsigned)moved;
                     q.idle_ns = 32;
@@ -207,14 +207,15 @@ __device__ __forceinline__ void worker_loop(const PlainParams &p, volatile Mirro
         }
         if constexpr (kStatsSmem) wstat_add(WS_BATCHES, 1u);
         else q.batches++;
-        relax_batch<Arcs, K>(p, q, ring, stage, valid, v, d);
+        relax_batch<Arcs, K, kSplit>(p, q, ring, stage, valid, v, d);
     }
 }
 
 // `grank`/`gsize`: this CTA's rank in, and the size of, the group of CTAs
 // that serves the query (the whole grid for a single-source launch).  K is
-// the number of 32-arc relaxation rounds a warp keeps in flight.
-template <class Arcs, int K>
+// the number of 32-arc relaxation rounds a warp keeps in flight; kSplit as
+// for relax_batch (true whenever the graph has pieces or light_heavy is on).
+template <class Arcs, int K, bool kSplit = true>
 __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank, unsigned gsize) {
     extern __shared__ uint2 smem[];
     volatile Mirror &mir = cta_mirror;
@@ -281,7 +282,7 @@ __device__ __forceinline__ void plain_body(const PlainParams &p, unsigned grank,
         __syncwarp();
     }
 
-    worker_loop<Arcs, K>(p, mir, ring, inb, stage, q);
+    worker_loop<Arcs, K, kSplit>(p, mir, ring, inb, stage, q);
 
     // ---- epilogue: statistics --------------------------------------------------
     unsigned long long pushed, l3_pushed, relaxed, improved, batches, idle;
