@@ -158,14 +158,15 @@ __global__ void interleave_kernel(const int *__restrict__ col, const int *__rest
         arcs[i] = make_int2(col[i], w[i]);
 }
 
-// Largest out-degree (out[0]) and largest weight (out[1]) of a CSR.
-__global__ void degree_weight_max_kernel(const int *__restrict__ row, int n, const int *__restrict__ w,
-                                         int64_t m, int *out) {
+// Largest out-degree of vertices [v0, v1) (out[0]) and largest weight of
+// arcs [a0, a1) (out[1]).
+__global__ void degree_weight_max_kernel(const int *__restrict__ row, int v0, int v1,
+                                         const int *__restrict__ w, int64_t a0, int64_t a1, int *out) {
     int dmax = 0, wmax = 0;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t v = tid; v < n; v += stride) dmax = max(dmax, row[v + 1] - row[v]);
-    for (int64_t e = tid; e < m; e += stride) wmax = max(wmax, w[e]);
+    for (int64_t v = v0 + tid; v < v1; v += stride) dmax = max(dmax, row[v + 1] - row[v]);
+    for (int64_t e = a0 + tid; e < a1; e += stride) wmax = max(wmax, w[e]);
     dmax = __reduce_max_sync(FULL, dmax);
     wmax = __reduce_max_sync(FULL, wmax);
     if ((threadIdx.x & 31) == 0) {
@@ -178,15 +179,16 @@ __global__ void degree_weight_max_kernel(const int *__restrict__ row, int n, con
 // low `wbits`, so one radix sort of all arcs orders them by vertex (keeping
 // the CSR offsets valid) and by weight within a vertex.  One warp per vertex,
 // lanes over its arcs, so a hub costs its degree / 32 steps.
-__global__ void arc_key_kernel(const int *__restrict__ row, int n, const int *__restrict__ w, int wbits,
-                               unsigned long long *keys) {
+// Keys of vertices [v0, v1); keys[i - a0] for arc i (a0 = row[v0]).
+__global__ void arc_key_kernel(const int *__restrict__ row, int v0, int v1, int64_t a0,
+                               const int *__restrict__ w, int wbits, unsigned long long *keys) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t v = warp; v < n; v += nwarps) {
+    for (int64_t v = v0 + warp; v < v1; v += nwarps) {
         const int b = row[v], e = row[v + 1];
         for (int i = b + lane; i < e; i += 32)
-            keys[i] = ((unsigned long long)v << wbits) | (unsigned)w[i];
+            keys[i - a0] = ((unsigned long long)v << wbits) | (unsigned)w[i];
     }
 }
 
@@ -529,8 +531,121 @@ namespace {
 
 // `h_row`: the same row offsets in host memory when the caller has them
 // (saves copying them back to find the heavy vertices), else null.
+// A vertex range [v0, v1) whose arcs [a0, a1) are sorted as one piece;
+// `ready`, if set, is an event recorded once the range's destinations and
+// weights (and the row offsets) are on the device.
+struct ArcRange {
+    int v0, v1;
+    int64_t a0, a1;
+    cudaEvent_t ready;
+};
+
+// Each vertex's arcs sorted by weight (light arcs, w < delta, then form a
+// prefix for any delta) and interleaved into arcs[], range by range, on the
+// legacy default stream.  A range whose largest vertex has more than
+// SPLIT_MIN arcs is sorted with one radix sort of (vertex, weight) keys,
+// which the skew of a power-law graph does not slow down; other ranges with
+// a segmented sort, which suits small degrees.  Ranges let the upload sort
+// one part of the graph while the next is still being copied (R-MAT-22
+// upload 21.4 -> 14.7 ms, 9.8 ms of it the PCIe copy).
+int build_arcs(int n, int64_t m, const int *d_row, const int *d_col, const int *d_w,
+               const std::vector<ArcRange> &ranges, int2 *arcs) {
+    int vbits = 1;
+    while (vbits < 31 && ((n - 1) >> vbits) != 0) vbits++;
+    int64_t max_arcs = 0;
+    for (const ArcRange &r : ranges) max_arcs = std::max<int64_t>(max_arcs, r.a1 - r.a0);
+    int *d_max = nullptr, *v_out = nullptr, *k32 = nullptr;
+    unsigned long long *k_in = nullptr, *k_out = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int rc = dev_alloc(&d_max, 2 * sizeof(int), 0, "alloc(max)");
+    if (!rc) rc = dev_alloc(&v_out, sizeof(int) * (size_t)m, 0, "alloc(sort values)");
+    for (size_t ri = 0; !rc && ri < ranges.size(); ri++) {
+        const ArcRange &r = ranges[ri];
+        if (r.a1 == r.a0) continue;
+        if (r.ready) rc = cuda_fail(cudaStreamWaitEvent(0, r.ready, 0), "wait range");
+        int maxes[2] = {0, 0};  // largest degree, largest weight in the range
+        if (!rc) rc = cuda_fail(cudaMemsetAsync(d_max, 0, 2 * sizeof(int), 0), "max init");
+        if (!rc) {
+            const int blocks = (int)std::min<int64_t>((r.a1 - r.a0 + 255) / 256, 148 * 8);
+            degree_weight_max_kernel<<<blocks, 256>>>(d_row, r.v0, r.v1, d_w, r.a0, r.a1, d_max);
+            rc = cuda_fail(cudaGetLastError(), "max launch");
+        }
+        if (!rc) rc = cuda_fail(cudaMemcpy(maxes, d_max, sizeof(maxes), cudaMemcpyDeviceToHost),
+                                "D2H max");
+        const int cnt = (int)(r.a1 - r.a0);
+        size_t need = 0;
+        if (!rc && maxes[0] > SPLIT_MIN) {
+            int wbits = 1;
+            while (wbits < 31 && (maxes[1] >> wbits) != 0) wbits++;
+            if (!k_in) rc = dev_alloc(&k_in, sizeof(unsigned long long) * (size_t)max_arcs, 0, "alloc(sort keys)");
+            if (!rc && !k_out)
+                rc = dev_alloc(&k_out, sizeof(unsigned long long) * (size_t)max_arcs, 0, "alloc(sort keys)");
+            if (!rc)
+                rc = cuda_fail(cub::DeviceRadixSort::SortPairs(nullptr, need, k_in, k_out, d_col + r.a0,
+                                                               v_out + r.a0, cnt, 0, vbits + wbits),
+                               "radix sort size");
+            if (!rc && need > tmp_bytes) {
+                dev_free(tmp, 0);
+                tmp = nullptr;
+                tmp_bytes = need;
+                rc = dev_alloc(&tmp, tmp_bytes, 0, "alloc(sort)");
+            }
+            if (!rc) {
+                const int blocks = (int)std::min<int64_t>(((int64_t)(r.v1 - r.v0) * 32 + 255) / 256, 148 * 16);
+                arc_key_kernel<<<blocks, 256>>>(d_row, r.v0, r.v1, r.a0, d_w, wbits, k_in);
+                rc = cuda_fail(cudaGetLastError(), "arc key launch");
+            }
+            size_t have = tmp_bytes;
+            if (!rc)
+                rc = cuda_fail(cub::DeviceRadixSort::SortPairs(tmp, have, k_in, k_out, d_col + r.a0,
+                                                               v_out + r.a0, cnt, 0, vbits + wbits),
+                               "radix sort arcs");
+            if (!rc) {
+                const int blocks = (int)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
+                interleave_keyed_kernel<<<blocks, 256>>>(v_out + r.a0, k_out, (1ull << wbits) - 1ull,
+                                                         arcs + r.a0, cnt);
+                rc = cuda_fail(cudaGetLastError(), "interleave launch");
+            }
+        } else if (!rc) {
+            // Segments address the arrays by absolute arc index (the row
+            // offsets), so the keys buffer spans all m arcs.
+            if (!k32) rc = dev_alloc(&k32, sizeof(int) * (size_t)m, 0, "alloc(sort keys)");
+            if (!rc)
+                rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(nullptr, need, d_w, k32, d_col, v_out,
+                                                                   (int)m, r.v1 - r.v0, d_row + r.v0,
+                                                                   d_row + r.v0 + 1),
+                               "sort size");
+            if (!rc && need > tmp_bytes) {
+                dev_free(tmp, 0);
+                tmp = nullptr;
+                tmp_bytes = need;
+                rc = dev_alloc(&tmp, tmp_bytes, 0, "alloc(sort)");
+            }
+            size_t have = tmp_bytes;
+            if (!rc)
+                rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(tmp, have, d_w, k32, d_col, v_out,
+                                                                   (int)m, r.v1 - r.v0, d_row + r.v0,
+                                                                   d_row + r.v0 + 1),
+                               "sort arcs");
+            if (!rc) {
+                const int blocks = (int)std::min<int64_t>((cnt + 255) / 256, 148 * 16);
+                interleave_kernel<<<blocks, 256>>>(v_out + r.a0, k32 + r.a0, arcs + r.a0, cnt);
+                rc = cuda_fail(cudaGetLastError(), "interleave launch");
+            }
+        }
+    }
+    dev_free(d_max, 0);
+    dev_free(v_out, 0);
+    dev_free(k32, 0);
+    dev_free(k_in, 0);
+    dev_free(k_out, 0);
+    dev_free(tmp, 0);
+    return rc;
+}
+
 int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int *d_w,
-                mlmq_graph **out) {
+                const std::vector<ArcRange> &ranges, mlmq_graph **out) {
     if (!out || n <= 0 || m < 0 || m >= INT_MAX || !d_row || (m > 0 && (!d_col || !d_w)))
         return MLMQ_ERR_ARG;
     auto *g = new (std::nothrow) mlmq_graph;
@@ -546,81 +661,7 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
     // graph can be built while a server kernel runs).
     int rc = cuda_fail(cudaGetDevice(&g->device), "cudaGetDevice");
     if (!rc) rc = dev_alloc(&g->d_arcs, sizeof(int2) * (size_t)(m > 0 ? m : 1), 0, "alloc(arcs)");
-    // Each vertex's arcs sorted by weight (light arcs, w < delta, then form a
-    // prefix for any delta), then interleaved.  A segmented sort suits
-    // graphs of small degrees; on a skewed graph (a vertex above SPLIT_MIN
-    // arcs) one radix sort of (vertex, weight) keys over all arcs is faster
-    // (R-MAT-22 upload 21.4 -> 18.9 ms, 9.8 ms of it the PCIe copy).
-    int maxes[2] = {0, 0};  // largest degree, largest weight
-    if (!rc && m > 0) {
-        int *d_max = nullptr;
-        rc = dev_alloc(&d_max, 2 * sizeof(int), 0, "alloc(max)");
-        if (!rc) rc = cuda_fail(cudaMemsetAsync(d_max, 0, 2 * sizeof(int), 0), "max init");
-        if (!rc) {
-            const int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 8);
-            degree_weight_max_kernel<<<blocks, 256>>>(d_row, n, d_w, m, d_max);
-            rc = cuda_fail(cudaGetLastError(), "max launch");
-        }
-        if (!rc) rc = cuda_fail(cudaMemcpy(maxes, d_max, sizeof(maxes), cudaMemcpyDeviceToHost),
-                                "D2H max");
-        dev_free(d_max, 0);
-    }
-    if (!rc && m > 0 && maxes[0] > SPLIT_MIN) {
-        int wbits = 1, vbits = 1;
-        while (wbits < 31 && (maxes[1] >> wbits) != 0) wbits++;
-        while (vbits < 31 && ((n - 1) >> vbits) != 0) vbits++;
-        unsigned long long *k_in = nullptr, *k_out = nullptr;
-        int *v_out = nullptr;
-        void *tmp = nullptr;
-        size_t tmp_bytes = 0;
-        rc = cuda_fail(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k_in, k_out, d_col, v_out,
-                                                       (int)m, 0, vbits + wbits),
-                       "radix sort size");
-        if (!rc) rc = dev_alloc(&tmp, tmp_bytes, 0, "alloc(sort)");
-        if (!rc) rc = dev_alloc(&k_in, sizeof(unsigned long long) * (size_t)m, 0, "alloc(sort keys)");
-        if (!rc) rc = dev_alloc(&k_out, sizeof(unsigned long long) * (size_t)m, 0, "alloc(sort keys)");
-        if (!rc) rc = dev_alloc(&v_out, sizeof(int) * (size_t)m, 0, "alloc(sort values)");
-        if (!rc) {
-            const int blocks = (int)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, 148 * 16);
-            arc_key_kernel<<<blocks, 256>>>(d_row, n, d_w, wbits, k_in);
-            rc = cuda_fail(cudaGetLastError(), "arc key launch");
-        }
-        if (!rc)
-            rc = cuda_fail(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, d_col, v_out,
-                                                           (int)m, 0, vbits + wbits),
-                           "radix sort arcs");
-        if (!rc) {
-            const int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
-            interleave_keyed_kernel<<<blocks, 256>>>(v_out, k_out, (1ull << wbits) - 1ull, g->d_arcs, m);
-            rc = cuda_fail(cudaGetLastError(), "interleave launch");
-        }
-        dev_free(tmp, 0);
-        dev_free(k_in, 0);
-        dev_free(k_out, 0);
-        dev_free(v_out, 0);
-    } else if (!rc && m > 0) {
-        int *k_out = nullptr, *v_out = nullptr;
-        void *tmp = nullptr;
-        size_t tmp_bytes = 0;
-        rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, d_w, k_out, d_col, v_out,
-                                                           (int)m, n, d_row, d_row + 1),
-                       "sort size");
-        if (!rc) rc = dev_alloc(&tmp, tmp_bytes, 0, "alloc(sort)");
-        if (!rc) rc = dev_alloc(&k_out, sizeof(int) * (size_t)m, 0, "alloc(sort keys)");
-        if (!rc) rc = dev_alloc(&v_out, sizeof(int) * (size_t)m, 0, "alloc(sort values)");
-        if (!rc)
-            rc = cuda_fail(cub::DeviceSegmentedSort::SortPairs(tmp, tmp_bytes, d_w, k_out, d_col, v_out,
-                                                               (int)m, n, d_row, d_row + 1),
-                           "sort arcs");
-        if (!rc) {
-            int blocks = (int)std::min<int64_t>((m + 255) / 256, 148 * 16);
-            interleave_kernel<<<blocks, 256>>>(v_out, k_out, g->d_arcs, m);
-            rc = cuda_fail(cudaGetLastError(), "interleave launch");
-        }
-        dev_free(tmp, 0);
-        dev_free(k_out, 0);
-        dev_free(v_out, 0);
-    }
+    if (!rc && m > 0) rc = build_arcs(n, m, d_row, d_col, d_w, ranges, g->d_arcs);
     // Heavy vertices (more than SPLIT_MIN arcs) are found on the device; at
     // most m / (SPLIT_MIN + 1) exist.  Their pieces are laid out on the host
     // in vertex order.
@@ -712,7 +753,8 @@ int wrap_device(int n, int64_t m, const int *d_row, const int *d_col, const int 
 
 extern "C" int mlmq_graph_wrap_device(int n, int64_t m, const int *d_row, const int *d_col,
                                       const int *d_w, mlmq_graph **out) {
-    return wrap_device(n, m, d_row, d_col, d_w, out);
+    if (n <= 0 || m < 0) return MLMQ_ERR_ARG;
+    return wrap_device(n, m, d_row, d_col, d_w, {ArcRange{0, n, 0, m, nullptr}}, out);
 }
 
 extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
@@ -720,20 +762,55 @@ extern "C" int mlmq_graph_upload(int n, int64_t m, const int *row, const int *co
     if (!out || n <= 0 || m < 0 || m >= INT_MAX || !row || (m > 0 && (!col || !w)))
         return MLMQ_ERR_ARG;
     if (row[0] != 0 || row[n] != m) return MLMQ_ERR_ARG;
+    // The arcs go over in ranges of whole vertices, on a copy stream, and
+    // each range is sorted as soon as it has arrived: the sort of one range
+    // runs beside the copy of the next (a large graph: up to 8 ranges of
+    // at least 4M arcs).
+    std::vector<ArcRange> ranges;
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(8, m / (4 << 20)));
+    int v = 0;
+    for (int64_t k = 1; k <= parts; k++) {
+        const int64_t target = m * k / parts;
+        const int v1 = k == parts ? n
+                                  : (int)(std::upper_bound(row + v, row + n, target) - row) - 1;
+        const int vend = std::max(v1, v);
+        if (vend > v || k == parts) ranges.push_back(ArcRange{v, vend, row[v], row[vend], nullptr});
+        v = vend;
+    }
     int *d_row = nullptr, *d_col = nullptr, *d_w = nullptr;
+    cudaStream_t cs = nullptr;
     int rc = dev_alloc(&d_row, sizeof(int) * ((size_t)n + 1), 0, "alloc(row)");
     if (!rc && m > 0) rc = dev_alloc(&d_col, sizeof(int) * (size_t)m, 0, "alloc(col)");
     if (!rc && m > 0) rc = dev_alloc(&d_w, sizeof(int) * (size_t)m, 0, "alloc(w)");
-    if (!rc) rc = cuda_fail(cudaMemcpy(d_row, row, sizeof(int) * ((size_t)n + 1),
-                                       cudaMemcpyHostToDevice), "H2D row");
-    if (!rc && m > 0)
-        rc = cuda_fail(cudaMemcpy(d_col, col, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
+    // The copy stream starts after the allocations (ordered on stream 0).
+    cudaEvent_t allocated = nullptr;
+    if (!rc) rc = cuda_fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "copy stream");
+    if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming), "event");
+    if (!rc) rc = cuda_fail(cudaEventRecord(allocated, 0), "event");
+    if (!rc) rc = cuda_fail(cudaStreamWaitEvent(cs, allocated, 0), "event wait");
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(d_row, row, sizeof(int) * ((size_t)n + 1),
+                                            cudaMemcpyHostToDevice, cs), "H2D row");
+    for (ArcRange &r : ranges) {
+        if (rc || r.a1 == r.a0) continue;
+        const size_t off = (size_t)r.a0, bytes = sizeof(int) * (size_t)(r.a1 - r.a0);
+        rc = cuda_fail(cudaMemcpyAsync(d_col + off, col + off, bytes, cudaMemcpyHostToDevice, cs),
                        "H2D col");
-    if (!rc && m > 0)
-        rc = cuda_fail(cudaMemcpy(d_w, w, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice),
-                       "H2D w");
+        if (!rc) rc = cuda_fail(cudaMemcpyAsync(d_w + off, w + off, bytes, cudaMemcpyHostToDevice, cs),
+                                "H2D w");
+        if (!rc) rc = cuda_fail(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming), "event");
+        if (!rc) rc = cuda_fail(cudaEventRecord(r.ready, cs), "event");
+    }
+    // With no arcs the row offsets still have to arrive before the build.
+    if (!rc && m == 0) rc = cuda_fail(cudaStreamSynchronize(cs), "H2D row");
     mlmq_graph *g = nullptr;
-    if (!rc) rc = wrap_device(n, m, d_row, d_col, d_w, &g);
+    if (!rc) rc = wrap_device(n, m, d_row, d_col, d_w, ranges, &g);
+    if (cs) {
+        cudaStreamSynchronize(cs);  // copies end before their buffers are freed
+        cudaStreamDestroy(cs);
+    }
+    for (ArcRange &r : ranges)
+        if (r.ready) cudaEventDestroy(r.ready);
+    if (allocated) cudaEventDestroy(allocated);
     dev_free(d_col, 0);
     dev_free(d_w, 0);
     if (rc) {

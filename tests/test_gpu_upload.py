@@ -25,12 +25,20 @@ def _check_arcs(g, col, w):
         "a vertex's arcs are not a permutation of its input arcs"
 
 
-@pytest.mark.parametrize("kind", ["rmat", "rmat_wide_weights", "grid"])
+@pytest.mark.parametrize("kind", ["rmat", "rmat_wide_weights", "grid", "rmat_ranges", "grid_ranges"])
 def test_uploaded_arcs_are_each_vertex_arcs_sorted_by_weight(kind):
+    # *_ranges: above 8M arcs the upload copies and sorts the graph in
+    # ranges of vertices, each sorted while the next is copied
     if kind == "rmat":
         g = HostGraph.rmat(16, 16, seed=5)
     elif kind == "rmat_wide_weights":
         g = HostGraph.rmat(15, 16, wmin=0, wmax=(1 << 31) - 2, seed=6)
+    elif kind == "rmat_ranges":
+        g = HostGraph.rmat(20, 16, seed=9)
+        assert g.m >= 8 << 20
+    elif kind == "grid_ranges":
+        g = HostGraph.grid(1600, 1500, seed=10)
+        assert g.m >= 8 << 20
     else:
         g = HostGraph.grid(300, 200, seed=7)
     dg = DeviceGraph.upload(g)
