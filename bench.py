@@ -124,18 +124,30 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel, workload):
-    """Per-launch DRAM bytes from the committed ncu summary, if captured."""
+def ncu_traffic(kernel, workload, delta=None):
+    """Per-launch DRAM bytes from the committed ncu summary, if captured:
+    (bytes, delta of the captured configuration or None).  A workload may
+    have captures at several bucket widths (`delta=N` after the bytes); the
+    one at the tuned delta is taken, else the nearest."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    found = []
     try:
         with open(path) as f:
             for line in f:
                 parts = line.split()
                 if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
-                    return float(parts[2])
+                    tag = None
+                    if len(parts) >= 4 and parts[3].startswith("delta="):
+                        tag = int(parts[3][len("delta="):])
+                    found.append((float(parts[2]), tag))
     except OSError:
         pass
-    return None
+    if not found:
+        return None, None
+    if delta is None or all(t is None for _, t in found):
+        return found[0]
+    tagged = [f for f in found if f[1] is not None]
+    return min(tagged, key=lambda f: abs(f[1] - int(delta)))
 
 
 class ClockSampler:
@@ -406,7 +418,7 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
     launch_s = per_query_ms / 1e3
     achieved_gbs = float(np.sum(np.tile(bytes_q, steps)) / np.sum(launch_s) / 1e9)
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic("sssp_plain_kernel", name)
+    traffic, traffic_delta = ncu_traffic("sssp_plain_kernel", name, cfg.delta)
     stats = solver.stats()
     solver.close()
 
@@ -478,6 +490,8 @@ def plain_arm(args, name, g, srcs, rep, local, steps, warmup, cpu_baseline, e2e_
         "work_per_step": int(work_step),
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                      "frac": achieved_gbs / peak, "traffic": traffic,
+                     "traffic_capture": (f"one ncu capture at delta {traffic_delta}"
+                                         if traffic_delta is not None else "one ncu capture"),
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel": "sssp_plain_kernel",
                      "algorithmic_bytes_per_launch": float(np.mean(bytes_q))},
@@ -630,7 +644,7 @@ def batched_arm(args, rep, local):
                        "p99": float(np.percentile(step_ms, 99)),
                        "note": "every query of a batch completes within its launch"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic("sssp_batch_kernel", "c4"),
+                     "frac": achieved / peak, "traffic": ncu_traffic("sssp_batch_kernel", "c4")[0],
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel": "sssp_batch_kernel",
                      "algorithmic_bytes_per_launch": bytes_step},

@@ -38,9 +38,23 @@ def test_clock_summary_flags_thermal_slowdown_and_empty_log():
 def test_peak_and_traffic_lookups():
     peak, kind = bench.measured_peak()
     assert peak > 1000 and kind in ("measured", "fallback")
-    t = bench.ncu_traffic("sssp_plain_kernel", "c2")
+    t, _ = bench.ncu_traffic("sssp_plain_kernel", "c2")
     assert t is None or t > 0
-    assert bench.ncu_traffic("no_such_kernel", "c2") is None
+    assert bench.ncu_traffic("no_such_kernel", "c2") == (None, None)
+
+
+def test_traffic_lookup_takes_the_capture_at_the_nearest_delta(tmp_path, monkeypatch):
+    (tmp_path / "profiles").mkdir()
+    (tmp_path / "profiles" / "ncu_traffic.txt").write_text(
+        "# comment\n"
+        "k w 100 delta=50000\n"
+        "k w 300 delta=200000\n"
+        "k2 w 7\n")
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.ncu_traffic("k", "w", 55389) == (100.0, 50000)
+    assert bench.ncu_traffic("k", "w", 221558) == (300.0, 200000)
+    assert bench.ncu_traffic("k", "w") == (100.0, 50000)
+    assert bench.ncu_traffic("k2", "w", 12345) == (7.0, None)
 
 
 def test_default_arguments(monkeypatch):
