@@ -229,8 +229,13 @@ typedef struct mlmq_solver mlmq_solver;
  * memory still in use is not affected. */
 int mlmq_release_cached(void);
 
-/* Copies a host CSR to the current device (pinned staging) and builds the
- * interleaved {dst, weight} arc array the kernels read. */
+/* Copies a host CSR to the current device and builds the interleaved
+ * {dst, weight} arc array the kernels read (each vertex's arcs sorted by
+ * weight), the vertex tiles and the pieces of split vertices; returns when
+ * the graph is complete.  A large graph's arcs go over in ranges of whole
+ * vertices on a copy stream of its own, each range sorted while the next is
+ * copied; with page-locked host arrays the copies run at PCIe speed (the
+ * driver stages pageable ones). */
 int mlmq_graph_upload(int n, int64_t m, const int *row, const int *col, const int *w,
                       mlmq_graph **out);
 /* Wraps a caller-owned device CSR (not copied; must outlive the graph). */
